@@ -1,0 +1,340 @@
+"""The ``droid_backends`` operator surface of HI-SLAM2, on the B200 kernels.
+
+Same names, positional signatures, return conventions and contiguity errors as
+the reference binding (``src/droid.cpp:116-341``); every op validates dtype,
+device and shape as well (the reference leaves those undefined) and launches
+on the current PyTorch stream.  All compute runs in ``libhislam2_b200.so``.
+"""
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+_DTYPES = {torch.float32: _lib.HS2_F32, torch.float16: _lib.HS2_F16,
+           torch.bfloat16: _lib.HS2_BF16, torch.float64: _lib.HS2_F64}
+
+
+def _contig(name, t):
+    # message of the reference's CHECK_CONTIGUOUS (src/droid.cpp:116)
+    if not t.is_contiguous():
+        raise RuntimeError("%s must be contiguous" % name)
+
+
+def _cuda(name, t, device=None):
+    if not isinstance(t, torch.Tensor):
+        raise RuntimeError("%s must be a torch.Tensor" % name)
+    if not t.is_cuda:
+        raise RuntimeError("%s must be a CUDA tensor" % name)
+    if device is not None and t.device != device:
+        raise RuntimeError("%s is on %s, expected %s" % (name, t.device, device))
+
+
+def _dtype(name, t, *dtypes):
+    if t.dtype not in dtypes:
+        raise RuntimeError("%s must have dtype %s (got %s)" % (name, " or ".join(map(str, dtypes)), t.dtype))
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+def _raise_device_errors(bits, op):
+    if bits & _lib.HS2_DEV_BAD_INDEX:
+        raise RuntimeError("%s: an edge index is out of range (ii/jj outside the buffers or >= t1)" % op)
+    if bits & _lib.HS2_DEV_BAD_ETA:
+        raise RuntimeError("%s: eta must have M or 1 rows (M = number of distinct depth frames)" % op)
+
+
+# --------------------------------------------------------------------------- ba
+def ba_workspace_bytes(num_poses, num_disps, ht, wd, num_edges, t0, t1, motion_only):
+    n = ctypes.c_size_t(0)
+    _lib.check(_lib.load().hs2_ba_workspace_size(num_poses, num_disps, ht, wd, num_edges, t0, t1,
+                                                 int(bool(motion_only)), ctypes.byref(n)),
+               "ba_workspace_size")
+    return n.value
+
+
+def _ba_check(poses, disps, intrinsics, targets, weights, eta, ii, jj):
+    for name, t in (("targets", targets), ("weights", weights), ("poses", poses), ("disps", disps),
+                    ("intrinsics", intrinsics), ("ii", ii), ("jj", jj)):
+        _contig(name, t)
+    dev = poses.device
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("targets", targets),
+                    ("weights", weights), ("eta", eta), ("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("targets", targets),
+                    ("weights", weights), ("eta", eta)):
+        _dtype(name, t, torch.float32)
+    _dtype("ii", ii, torch.int64)
+    _dtype("jj", jj, torch.int64)
+    if poses.dim() != 2 or poses.shape[1] != 7:
+        raise RuntimeError("poses must be [N, 7] (got %s)" % tuple(poses.shape))
+    if disps.dim() != 3:
+        raise RuntimeError("disps must be [N, H, W] (got %s)" % tuple(disps.shape))
+    if intrinsics.numel() < 4:
+        raise RuntimeError("intrinsics must hold fx, fy, cx, cy")
+    E = ii.numel()
+    ht, wd = disps.shape[1], disps.shape[2]
+    if jj.numel() != E:
+        raise RuntimeError("ii and jj must have the same length")
+    for name, t in (("targets", targets), ("weights", weights)):
+        if tuple(t.shape) != (E, 2, ht, wd):
+            raise RuntimeError("%s must be [num_edges, 2, H, W] = %s (got %s)" % (name, (E, 2, ht, wd),
+                                                                                 tuple(t.shape)))
+    if eta.numel() % (ht * wd) != 0:
+        raise RuntimeError("eta must hold whole [H, W] maps (got %s)" % tuple(eta.shape))
+
+
+def ba(poses, disps, intrinsics, *args, disps_sens=None):
+    """Dense bundle adjustment, ``droid_backends.ba`` (reference ``src/droid.cpp:141-168``).
+
+    ``ba(poses, disps, intrinsics, targets, weights, eta, ii, jj, t0, t1, iterations,
+    lm, ep, motion_only) -> [dx, dz, dzcov]``; the 15-argument form with
+    ``disps_sens`` after ``intrinsics`` is accepted with ``disps_sens=None``.
+    ``poses`` and ``disps`` are updated in place.  ``dz`` is None when
+    ``motion_only``; ``dzcov`` is always None (undefined in the reference).
+    """
+    if len(args) == 12:
+        disps_sens, args = args[0], args[1:]
+    if len(args) != 11:
+        raise TypeError("ba() takes 14 positional arguments (15 with disps_sens), got %d" % (3 + len(args)))
+    targets, weights, eta, ii, jj, t0, t1, iterations, lm, ep, motion_only = args
+    if disps_sens is not None:
+        raise RuntimeError("ba: disps_sens is not part of HI-SLAM2's bundle adjustment; pass None")
+    _ba_check(poses, disps, intrinsics, targets, weights, eta, ii, jj)
+    eta = eta.contiguous()
+    dev = poses.device
+    t0, t1, iterations = int(t0), int(t1), int(iterations)
+    motion_only = bool(motion_only)
+    K, (Kd, ht, wd), E = poses.shape[0], disps.shape, ii.numel()
+    P = t1 - t0
+    ws_bytes = ba_workspace_bytes(K, Kd, ht, wd, E, t0, t1, motion_only)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    S = max(1, min(min(K, Kd), P + E))
+    dx = torch.zeros(max(P, 0), 6, dtype=torch.float32, device=dev)
+    dz = torch.zeros(S, ht * wd, dtype=torch.float32, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    lib = _lib.load()
+    _lib.check(lib.hs2_ba(_ptr(poses), K, _ptr(disps), Kd, ht, wd, _ptr(intrinsics), _ptr(targets),
+                          _ptr(weights), _ptr(eta), eta.numel() // (ht * wd), _ptr(ii), _ptr(jj), E, t0, t1,
+                          iterations, float(lm), float(ep), int(motion_only), _ptr(dx), _ptr(dz), S,
+                          _ptr(info), _ptr(ws), ws_bytes, _stream(dev)), "ba")
+    h = info.cpu()
+    _raise_device_errors(int(h[0]), "ba")
+    M = int(h[1])
+    return [dx, None if motion_only else dz[:M], None]
+
+
+def ba_reduced_system(poses, disps, intrinsics, targets, weights, eta, ii, jj, t0, t1, motion_only=False):
+    """The reduced camera system (A - S, b - v) of one linearisation at the given state,
+    before damping, as float64 CUDA tensors ``[6P, 6P]`` and ``[6P]`` (diagnostic)."""
+    _ba_check(poses, disps, intrinsics, targets, weights, eta, ii, jj)
+    eta = eta.contiguous()
+    dev = poses.device
+    K, (Kd, ht, wd), E = poses.shape[0], disps.shape, ii.numel()
+    t0, t1 = int(t0), int(t1)
+    n = 6 * (t1 - t0)
+    ws_bytes = ba_workspace_bytes(K, Kd, ht, wd, E, t0, t1, motion_only)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    A = torch.zeros(n, n, dtype=torch.float64, device=dev)
+    b = torch.zeros(n, dtype=torch.float64, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_ba_reduced_system(
+        _ptr(poses), K, _ptr(disps), Kd, ht, wd, _ptr(intrinsics), _ptr(targets), _ptr(weights), _ptr(eta),
+        eta.numel() // (ht * wd), _ptr(ii), _ptr(jj), E, t0, t1, int(bool(motion_only)), _ptr(A), _ptr(b),
+        _ptr(info), _ptr(ws), ws_bytes, _stream(dev)), "ba_reduced_system")
+    _raise_device_errors(int(info[0].item()), "ba_reduced_system")
+    return A, b
+
+
+def ba_keys(poses, disps, ii, jj, t0, t1):
+    """Integer keys of ``ba`` (unique depth frames, inverse index, Schur row lists).
+
+    Returns ``(kx, kk_exp, rows_ptr, rows)`` as int64 CPU tensors; see
+    ``hs2_ba_keys`` in ``include/hislam2_b200.h``.
+    """
+    _cuda("ii", ii)
+    _cuda("jj", jj, ii.device)
+    _dtype("ii", ii, torch.int64)
+    _dtype("jj", jj, torch.int64)
+    dev = ii.device
+    K, Kd, (ht, wd), E = poses.shape[0], disps.shape[0], disps.shape[1:], ii.numel()
+    P = t1 - t0
+    ws_bytes = ba_workspace_bytes(K, Kd, ht, wd, E, t0, t1, False)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    S = max(1, min(min(K, Kd), P + E))
+    kx = torch.zeros(S, dtype=torch.int32, device=dev)
+    kk = torch.zeros(max(1, P + E), dtype=torch.int32, device=dev)
+    rptr = torch.zeros(S + 1, dtype=torch.int32, device=dev)
+    rows = torch.zeros(max(1, P + E), dtype=torch.int32, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_ba_keys(K, Kd, ht, wd, _ptr(ii), _ptr(jj), E, t0, t1, _ptr(kx), _ptr(kk),
+                                       _ptr(rptr), _ptr(rows), _ptr(info), _ptr(ws), ws_bytes, _stream(dev)),
+               "ba_keys")
+    h = info.cpu()
+    _raise_device_errors(int(h[0]), "ba_keys")
+    M = int(h[1])
+    rptr = rptr[: M + 1].cpu().long()
+    return kx[:M].cpu().long(), kk[: P + E].cpu().long(), rptr, rows[: int(rptr[-1])].cpu().long()
+
+
+# -------------------------------------------------------------- frame_distance
+def frame_distance(poses, disps, intrinsics, ii, jj, beta):
+    """``droid_backends.frame_distance`` (reference ``src/droid.cpp:200-216``) -> dist [E]."""
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("ii", ii), ("jj", jj)):
+        _contig(name, t)
+    dev = poses.device
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics)):
+        _dtype(name, t, torch.float32)
+    _dtype("ii", ii, torch.int64)
+    _dtype("jj", jj, torch.int64)
+    if poses.dim() != 2 or poses.shape[1] != 7 or disps.dim() != 3:
+        raise RuntimeError("frame_distance: poses must be [N,7] and disps [N,H,W]")
+    if ii.numel() != jj.numel():
+        raise RuntimeError("frame_distance: ii and jj must have the same length")
+    E = ii.numel()
+    dist = torch.zeros(E, dtype=torch.float32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_frame_distance(_ptr(poses), poses.shape[0], _ptr(disps), disps.shape[0],
+                                              disps.shape[1], disps.shape[2], _ptr(intrinsics), _ptr(ii),
+                                              _ptr(jj), E, float(beta), _ptr(dist), _ptr(info), _stream(dev)),
+               "frame_distance")
+    if E:
+        _raise_device_errors(int(info.item()), "frame_distance")
+    return dist
+
+
+# ------------------------------------------------------------------ corr_index
+def _corr_dtype(name, t):
+    if t.dtype not in _DTYPES:
+        raise RuntimeError("%s: unsupported dtype %s" % (name, t.dtype))
+    return _DTYPES[t.dtype]
+
+
+def corr_index_forward(volume, coords, radius):
+    """``droid_backends.corr_index_forward`` (reference ``src/droid.cpp:254-264``) -> [corr]."""
+    _contig("volume", volume)
+    _contig("coords", coords)
+    _cuda("volume", volume)
+    _cuda("coords", coords, volume.device)
+    _dtype("coords", coords, torch.float32)
+    dt = _corr_dtype("volume", volume)
+    if volume.dim() != 5 or coords.dim() != 4 or coords.shape[1] != 2 or coords.shape[0] != volume.shape[0] \
+            or tuple(coords.shape[2:]) != tuple(volume.shape[1:3]):
+        raise RuntimeError("corr_index_forward: volume [N,H1,W1,H2,W2] and coords [N,2,H1,W1] expected, got %s "
+                           "and %s" % (tuple(volume.shape), tuple(coords.shape)))
+    n, h1, w1, h2, w2 = volume.shape
+    r = int(radius)
+    corr = torch.empty(n, 2 * r + 1, 2 * r + 1, h1, w1, dtype=volume.dtype, device=volume.device)
+    _lib.check(_lib.load().hs2_corr_index_forward(_ptr(volume), dt, n, h1, w1, h2, w2, _ptr(coords), r,
+                                                  _ptr(corr), _stream(volume.device)), "corr_index_forward")
+    return [corr]
+
+
+def corr_index_backward(volume, coords, corr_grad, radius):
+    """``droid_backends.corr_index_backward`` (reference ``src/droid.cpp:266-275``) -> [volume_grad]."""
+    _contig("volume", volume)
+    _contig("coords", coords)
+    _contig("corr_grad", corr_grad)
+    _cuda("volume", volume)
+    _cuda("coords", coords, volume.device)
+    _cuda("corr_grad", corr_grad, volume.device)
+    _dtype("coords", coords, torch.float32)
+    dt = _corr_dtype("volume", volume)
+    _dtype("corr_grad", corr_grad, volume.dtype)
+    n, h1, w1, h2, w2 = volume.shape
+    r = int(radius)
+    if tuple(corr_grad.shape) != (n, 2 * r + 1, 2 * r + 1, h1, w1):
+        raise RuntimeError("corr_index_backward: corr_grad must be %s (got %s)"
+                           % ((n, 2 * r + 1, 2 * r + 1, h1, w1), tuple(corr_grad.shape)))
+    volume_grad = torch.empty_like(volume)
+    _lib.check(_lib.load().hs2_corr_index_backward(_ptr(coords), _ptr(corr_grad), dt, n, h1, w1, h2, w2, r,
+                                                   _ptr(volume_grad), _stream(volume.device)),
+               "corr_index_backward")
+    return [volume_grad]
+
+
+# --------------------------------------------------------------------- altcorr
+def _altcorr_check(fmap1, fmap2, coords, ii, jj):
+    _contig("fmap1", fmap1)
+    _contig("fmap2", fmap2)
+    _contig("coords", coords)
+    dev = fmap1.device
+    for name, t in (("fmap1", fmap1), ("fmap2", fmap2), ("coords", coords), ("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+    _dtype("fmap2", fmap2, fmap1.dtype)
+    _dtype("coords", coords, torch.float32)
+    _dtype("ii", ii, torch.int64)
+    _dtype("jj", jj, torch.int64)
+    if fmap1.dim() != 5 or fmap2.dim() != 5 or coords.dim() != 5 or coords.shape[2] != 2:
+        raise RuntimeError("altcorr: fmaps [B,N,C,H,W] and coords [B,M,2,H,W] expected")
+    B, M = coords.shape[0], coords.shape[1]
+    if fmap1.shape[0] != B or fmap2.shape[0] != B or fmap1.shape[2] != fmap2.shape[2] \
+            or tuple(fmap1.shape[3:]) != tuple(coords.shape[3:]) or ii.numel() != M or jj.numel() != M:
+        raise RuntimeError("altcorr: inconsistent shapes fmap1 %s fmap2 %s coords %s ii %s jj %s" % (
+            tuple(fmap1.shape), tuple(fmap2.shape), tuple(coords.shape), tuple(ii.shape), tuple(jj.shape)))
+    return _corr_dtype("fmap1", fmap1)
+
+
+def altcorr_forward(fmap1, fmap2, coords, ii, jj, radius):
+    """``droid_backends.altcorr_forward`` (reference ``src/droid.cpp:277-289``) -> [corr].
+
+    corr is [B, M, 2r+1, 2r+1, H, W] with dim 2 along x, returned contiguous
+    (the reference returns the same values as a permuted view).
+    """
+    dt = _altcorr_check(fmap1, fmap2, coords, ii.contiguous(), jj.contiguous())
+    ii, jj = ii.contiguous(), jj.contiguous()
+    B, N1, C, H, W = fmap1.shape
+    N2, H2, W2 = fmap2.shape[1], fmap2.shape[3], fmap2.shape[4]
+    M = coords.shape[1]
+    r = int(radius)
+    corr = torch.empty(B, M, 2 * r + 1, 2 * r + 1, H, W, dtype=fmap1.dtype, device=fmap1.device)
+    info = torch.zeros(1, dtype=torch.int32, device=fmap1.device)
+    _lib.check(_lib.load().hs2_altcorr_forward(_ptr(fmap1), _ptr(fmap2), dt, B, N1, N2, C, H, W, H2, W2,
+                                               _ptr(coords), _ptr(ii), _ptr(jj), M, r, _ptr(corr), _ptr(info),
+                                               _stream(fmap1.device)), "altcorr_forward")
+    return [corr]
+
+
+def altcorr_backward(fmap1, fmap2, coords, ii, jj, grad, radius, scale=1.0):
+    """``droid_backends.altcorr_backward`` -> [fmap1_grad, fmap2_grad].
+
+    Positional order as HI-SLAM2 calls it (``hislam2/modules/corr.py:86``, which
+    the binding's swapped parameter names in ``src/droid.cpp:291-305`` cancel).
+    ``scale=1`` reproduces the reference operator, which leaves out the forward's
+    1/16; ``scale=1/16`` is the exact adjoint of :func:`altcorr_forward`.
+    """
+    dt = _altcorr_check(fmap1, fmap2, coords, ii, jj)
+    if dt == _lib.HS2_F64:
+        raise RuntimeError("altcorr_backward: float64 feature maps are not supported")
+    ii, jj = ii.contiguous(), jj.contiguous()
+    _cuda("grad", grad, fmap1.device)
+    _dtype("grad", grad, torch.float32)
+    grad = grad.contiguous()
+    B, N1, C, H, W = fmap1.shape
+    N2, H2, W2 = fmap2.shape[1], fmap2.shape[3], fmap2.shape[4]
+    M = coords.shape[1]
+    r = int(radius)
+    if tuple(grad.shape) != (B, M, 2 * r + 1, 2 * r + 1, H, W):
+        raise RuntimeError("altcorr_backward: grad must be %s" % ((B, M, 2 * r + 1, 2 * r + 1, H, W),))
+    lib = _lib.load()
+    nbytes = ctypes.c_size_t(0)
+    _lib.check(lib.hs2_altcorr_backward_workspace_size(dt, B, N1, N2, C, H, W, H2, W2, ctypes.byref(nbytes)),
+               "altcorr_backward_workspace_size")
+    ws = torch.empty(max(1, nbytes.value), dtype=torch.uint8, device=fmap1.device)
+    g1 = torch.empty_like(fmap1)
+    g2 = torch.empty_like(fmap2)
+    info = torch.zeros(1, dtype=torch.int32, device=fmap1.device)
+    _lib.check(lib.hs2_altcorr_backward(_ptr(fmap1), _ptr(fmap2), dt, B, N1, N2, C, H, W, H2, W2, _ptr(coords),
+                                        _ptr(ii), _ptr(jj), M, _ptr(grad), r, float(scale), _ptr(g1), _ptr(g2),
+                                        _ptr(info), _ptr(ws), nbytes.value, _stream(fmap1.device)),
+               "altcorr_backward")
+    return [g1, g2]

@@ -1,0 +1,332 @@
+// altcorr_forward / altcorr_backward: correlation windows computed on the fly
+// from feature maps, without materialising the all-pairs volume
+// (reference: src/altcorr_kernel.cu:25-225).
+//
+// Forward: a CTA owns 32 consecutive pixels of one (batch, correlation m).
+// Each work item (pixel, window row) forms the D = 2r+2 channel dot products of
+// that row in registers (FP32 accumulation over the C channels), the D x D
+// window lands in shared memory, and the bilinear blend writes the
+// (2r+1)^2 outputs with consecutive threads on consecutive pixels.  The /4 /4
+// feature scaling of the reference is applied once as 1/16 at the end.
+//
+// Backward: the adjoint of the bilinear blend is formed per window in shared
+// memory, then fmap1/fmap2 gradients are accumulated with FP32 atomics (a
+// frame may appear in several correlations).  `scale` multiplies every
+// product; the reference operator corresponds to scale = 1.
+#include "common.cuh"
+#include "profile.cuh"
+
+namespace hs2 {
+
+constexpr int kAcThreads = 256;
+constexpr int kAcPix = 32;    // pixels per CTA
+constexpr int kAcTaps = 16;   // taps per register chunk
+
+template <typename T>
+__global__ void __launch_bounds__(kAcThreads)
+altcorr_fwd_kernel(const T* __restrict__ fmap1, const T* __restrict__ fmap2, const float* __restrict__ coords,
+                   const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, T* __restrict__ corr,
+                   int N1, int N2, int C, int H, int W, int H2, int W2, int M, int r, int stride,
+                   int32_t* __restrict__ info) {
+  extern __shared__ float4 smem4[];
+  float4* geo = smem4;                                                   // [kAcPix]
+  float* win = reinterpret_cast<float*>(smem4) + 4 * kAcPix;            // [kAcPix][stride]
+
+  const int b = blockIdx.z;
+  const int m = blockIdx.y;
+  const int HW = H * W;
+  const int64_t HW2 = (int64_t)H2 * W2;
+  const int pix0 = blockIdx.x * kAcPix;
+  const int D = 2 * r + 2;
+  const int rd = 2 * r + 1;
+  const int64_t ix = ii[m], jx = jj[m];
+  const bool ok = ix >= 0 && ix < N1 && jx >= 0 && jx < N2;
+  if (!ok && threadIdx.x == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
+
+  const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
+  const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
+  for (int q = threadIdx.x; q < kAcPix; q += kAcThreads) {
+    const int pix = min(pix0 + q, HW - 1);
+    const float x = cx[pix], y = cy[pix];
+    const float fx = floorf(x), fy = floorf(y);
+    geo[q] = make_float4(x - fx, y - fy, __int_as_float((int)fx - r), __int_as_float((int)fy - r));
+  }
+  __syncthreads();
+
+  const T* f1 = fmap1 + ((int64_t)b * N1 + (ok ? ix : 0)) * C * HW;
+  const T* f2 = fmap2 + ((int64_t)b * N2 + (ok ? jx : 0)) * C * HW2;
+  for (int item = threadIdx.x; item < kAcPix * D; item += kAcThreads) {
+    const int py = item / kAcPix;
+    const int q = item - py * kAcPix;
+    const int pix = pix0 + q;
+    float* wrow = win + q * stride + py * D;
+    const float4 g = geo[q];
+    const int y1 = __float_as_int(g.w) + py;
+    const int xb = __float_as_int(g.z);
+    const bool row_ok = ok && pix < HW && y1 >= 0 && y1 < H2;
+    for (int c0 = 0; c0 < D; c0 += kAcTaps) {
+      float acc[kAcTaps];
+#pragma unroll
+      for (int k = 0; k < kAcTaps; ++k) acc[k] = 0.f;
+      if (row_ok) {
+        const T* a = f1 + pix;
+        const T* brow = f2 + (int64_t)y1 * W2;
+        for (int c = 0; c < C; ++c) {
+          const float av = to_f(a[(int64_t)c * HW]);
+          const T* bc = brow + (int64_t)c * HW2;
+#pragma unroll
+          for (int k = 0; k < kAcTaps; ++k) {
+            const int x1 = xb + c0 + k;
+            if (c0 + k < D && x1 >= 0 && x1 < W2) acc[k] += av * to_f(bc[x1]);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kAcTaps; ++k)
+        if (c0 + k < D) wrow[c0 + k] = acc[k] * 0.0625f;
+    }
+  }
+  __syncthreads();
+
+  const int nout = rd * rd;
+  T* out = corr + ((int64_t)b * M + m) * nout * HW;
+  for (int idx = threadIdx.x; idx < kAcPix * nout; idx += kAcThreads) {
+    const int o = idx / kAcPix;
+    const int q = idx - o * kAcPix;
+    const int pix = pix0 + q;
+    if (pix >= HW) continue;
+    const int a = o / rd;      // x offset (dim 2 of the output)
+    const int bb = o - a * rd; // y offset (dim 3 of the output)
+    const float4 g = geo[q];
+    const float* w = win + q * stride;
+    const float v = (1.f - g.x) * (1.f - g.y) * w[bb * D + a] + g.x * (1.f - g.y) * w[bb * D + a + 1] +
+                    (1.f - g.x) * g.y * w[(bb + 1) * D + a] + g.x * g.y * w[(bb + 1) * D + a + 1];
+    out[(int64_t)o * HW + pix] = from_f<T>(v);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kAcThreads)
+altcorr_bwd_kernel(const T* __restrict__ fmap1, const T* __restrict__ fmap2, const float* __restrict__ coords,
+                   const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, const float* __restrict__ grad,
+                   float* __restrict__ g1, float* __restrict__ g2, int N1, int N2, int C, int H, int W,
+                   int H2, int W2, int M, int r, int stride, float scale, int32_t* __restrict__ info) {
+  extern __shared__ float4 smem4[];
+  float4* geo = smem4;
+  float* gw = reinterpret_cast<float*>(smem4) + 4 * kAcPix;
+
+  const int b = blockIdx.z;
+  const int m = blockIdx.y;
+  const int HW = H * W;
+  const int64_t HW2 = (int64_t)H2 * W2;
+  const int pix0 = blockIdx.x * kAcPix;
+  const int npix = min(kAcPix, HW - pix0);
+  const int D = 2 * r + 2;
+  const int DD = D * D;
+  const int rd = 2 * r + 1;
+  const int64_t ix = ii[m], jx = jj[m];
+  if (!(ix >= 0 && ix < N1 && jx >= 0 && jx < N2)) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
+    return;
+  }
+  const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
+  const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
+  for (int q = threadIdx.x; q < npix; q += kAcThreads) {
+    const float x = cx[pix0 + q], y = cy[pix0 + q];
+    const float fx = floorf(x), fy = floorf(y);
+    geo[q] = make_float4(x - fx, y - fy, __int_as_float((int)fx - r), __int_as_float((int)fy - r));
+  }
+  __syncthreads();
+  // adjoint of the bilinear blend; grad layout [b, m, x-offset, y-offset, H, W]
+  const float* gr = grad + ((int64_t)b * M + m) * rd * rd * HW + pix0;
+  for (int idx = threadIdx.x; idx < npix * DD; idx += kAcThreads) {
+    const int t = idx / npix;
+    const int q = idx - t * npix;
+    const int py = t / D, px = t - (t / D) * D;
+    const float dx = geo[q].x, dy = geo[q].y;
+    float G = 0.f;
+    if (px < rd && py < rd) G += (1.f - dx) * (1.f - dy) * gr[(int64_t)(px * rd + py) * HW + q];
+    if (px > 0 && py < rd) G += dx * (1.f - dy) * gr[(int64_t)((px - 1) * rd + py) * HW + q];
+    if (px < rd && py > 0) G += (1.f - dx) * dy * gr[(int64_t)(px * rd + py - 1) * HW + q];
+    if (px > 0 && py > 0) G += dx * dy * gr[(int64_t)((px - 1) * rd + py - 1) * HW + q];
+    gw[q * stride + t] = G * scale;
+  }
+  __syncthreads();
+
+  const T* f1 = fmap1 + ((int64_t)b * N1 + ix) * C * HW;
+  const T* f2 = fmap2 + ((int64_t)b * N2 + jx) * C * HW2;
+  float* o1 = g1 + ((int64_t)b * N1 + ix) * C * HW;
+  float* o2 = g2 + ((int64_t)b * N2 + jx) * C * HW2;
+  // fmap1 gradient: one (pixel, channel) per item, sum over the window
+  for (int idx = threadIdx.x; idx < npix * C; idx += kAcThreads) {
+    const int c = idx / npix;
+    const int q = idx - c * npix;
+    const float4 g = geo[q];
+    const int xb = __float_as_int(g.z), yb = __float_as_int(g.w);
+    const T* bc = f2 + (int64_t)c * HW2;
+    float s = 0.f;
+    for (int t = 0; t < DD; ++t) {
+      const int py = t / D, px = t - (t / D) * D;
+      const int x1 = xb + px, y1 = yb + py;
+      if (x1 >= 0 && x1 < W2 && y1 >= 0 && y1 < H2) s += gw[q * stride + t] * to_f(bc[(int64_t)y1 * W2 + x1]);
+    }
+    atomicAdd(o1 + (int64_t)c * HW + pix0 + q, s);
+  }
+  // fmap2 gradient: one (pixel, tap) per item, loop over channels
+  for (int idx = threadIdx.x; idx < npix * DD; idx += kAcThreads) {
+    const int t = idx / npix;
+    const int q = idx - t * npix;
+    const float4 g = geo[q];
+    const int py = t / D, px = t - (t / D) * D;
+    const int x1 = __float_as_int(g.z) + px, y1 = __float_as_int(g.w) + py;
+    if (x1 < 0 || x1 >= W2 || y1 < 0 || y1 >= H2) continue;
+    const float G = gw[q * stride + t];
+    if (G == 0.f) continue;
+    const T* a = f1 + pix0 + q;
+    float* dst = o2 + (int64_t)y1 * W2 + x1;
+    for (int c = 0; c < C; ++c) atomicAdd(dst + (int64_t)c * HW2, G * to_f(a[(int64_t)c * HW]));
+  }
+}
+
+template <typename T>
+__global__ void cast_from_f32_kernel(const float* __restrict__ src, T* __restrict__ dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = from_f<T>(src[i]);
+}
+
+static int ac_stride(int radius) {
+  const int D = 2 * radius + 2;
+  int s = D * D;
+  if ((s & 1) == 0) s += 1;
+  return s;
+}
+
+static int ac_check(const char* op, int b, int n1, int n2, int c, int h, int w, int h2, int w2, int m,
+                    int radius) {
+  if (b < 0 || n1 < 0 || n2 < 0 || c <= 0 || h <= 0 || w <= 0 || h2 <= 0 || w2 <= 0 || m < 0 ||
+      radius < 0 || radius > 30 || m > 65535 || b > 65535) {
+    set_error("%s: bad sizes b=%d n1=%d n2=%d c=%d h=%d w=%d h2=%d w2=%d m=%d r=%d", op, b, n1, n2, c, h, w,
+              h2, w2, m, radius);
+    return HS2_ERR_INVALID;
+  }
+  return HS2_OK;
+}
+
+template <typename T>
+static int ac_fwd(const void* fmap1, const void* fmap2, int b, int n1, int n2, int c, int h, int w, int h2,
+                  int w2, const float* coords, const int64_t* ii, const int64_t* jj, int m, int radius,
+                  void* corr, int32_t* info, cudaStream_t s) {
+  const int stride = ac_stride(radius);
+  const size_t smem = (size_t)kAcPix * (stride * 4 + 16);
+  if (smem > 48 * 1024)
+    HS2_CUDA(cudaFuncSetAttribute(altcorr_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((h * w + kAcPix - 1) / kAcPix, m, b);
+  HS2_PROF("altcorr_fwd", s);
+  altcorr_fwd_kernel<T><<<grid, kAcThreads, smem, s>>>(
+      static_cast<const T*>(fmap1), static_cast<const T*>(fmap2), coords, ii, jj, static_cast<T*>(corr), n1,
+      n2, c, h, w, h2, w2, m, radius, stride, info);
+  HS2_LAUNCH_CHECK("altcorr_fwd_kernel");
+  return HS2_OK;
+}
+
+template <typename T>
+static int ac_bwd(const void* fmap1, const void* fmap2, int b, int n1, int n2, int c, int h, int w, int h2,
+                  int w2, const float* coords, const int64_t* ii, const int64_t* jj, int m, const float* grad,
+                  int radius, float scale, void* g1, void* g2, int32_t* info, void* ws, cudaStream_t s) {
+  const int64_t n1el = (int64_t)b * n1 * c * h * w;
+  const int64_t n2el = (int64_t)b * n2 * c * h2 * w2;
+  float* a1 = std::is_same<T, float>::value ? static_cast<float*>(g1) : static_cast<float*>(ws);
+  float* a2 = std::is_same<T, float>::value ? static_cast<float*>(g2) : static_cast<float*>(ws) + n1el;
+  HS2_CUDA(cudaMemsetAsync(a1, 0, n1el * sizeof(float), s));
+  HS2_CUDA(cudaMemsetAsync(a2, 0, n2el * sizeof(float), s));
+  const int stride = ac_stride(radius);
+  const size_t smem = (size_t)kAcPix * (stride * 4 + 16);
+  if (smem > 48 * 1024)
+    HS2_CUDA(cudaFuncSetAttribute(altcorr_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (m > 0 && b > 0) {
+    dim3 grid((h * w + kAcPix - 1) / kAcPix, m, b);
+    HS2_PROF("altcorr_bwd", s);
+    altcorr_bwd_kernel<T><<<grid, kAcThreads, smem, s>>>(
+        static_cast<const T*>(fmap1), static_cast<const T*>(fmap2), coords, ii, jj, grad, a1, a2, n1, n2, c, h,
+        w, h2, w2, m, radius, stride, scale, info);
+    HS2_LAUNCH_CHECK("altcorr_bwd_kernel");
+  }
+  if (!std::is_same<T, float>::value) {
+    if (n1el) {
+      cast_from_f32_kernel<T><<<1184, 256, 0, s>>>(a1, static_cast<T*>(g1), n1el);
+      HS2_LAUNCH_CHECK("cast_from_f32_kernel");
+    }
+    if (n2el) {
+      cast_from_f32_kernel<T><<<1184, 256, 0, s>>>(a2, static_cast<T*>(g2), n2el);
+      HS2_LAUNCH_CHECK("cast_from_f32_kernel");
+    }
+  }
+  return HS2_OK;
+}
+
+}  // namespace hs2
+
+extern "C" int hs2_altcorr_forward(const void* fmap1, const void* fmap2, int dtype, int b, int n1, int n2,
+                                   int c, int h, int w, int h2, int w2, const float* coords, const int64_t* ii,
+                                   const int64_t* jj, int m, int radius, void* corr, int32_t* info,
+                                   hs2_stream_t stream) {
+  using namespace hs2;
+  int rc = ac_check("altcorr_forward", b, n1, n2, c, h, w, h2, w2, m, radius);
+  if (rc) return rc;
+  if (m == 0 || b == 0) return HS2_OK;
+  if ((rc = bind_device(corr))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (dtype) {
+    case HS2_F32: return ac_fwd<float>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case HS2_F16: return ac_fwd<__half>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case HS2_BF16:
+      return ac_fwd<__nv_bfloat16>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case HS2_F64: return ac_fwd<double>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+  }
+  set_error("altcorr_forward: unsupported dtype %d", dtype);
+  return HS2_ERR_DTYPE;
+}
+
+extern "C" int hs2_altcorr_backward_workspace_size(int dtype, int b, int n1, int n2, int c, int h, int w,
+                                                   int h2, int w2, size_t* bytes) {
+  using namespace hs2;
+  if (!bytes) return HS2_ERR_INVALID;
+  if (dtype == HS2_F32) {
+    *bytes = 0;
+    return HS2_OK;
+  }
+  *bytes = ((size_t)b * n1 * c * h * w + (size_t)b * n2 * c * h2 * w2) * sizeof(float);
+  return HS2_OK;
+}
+
+extern "C" int hs2_altcorr_backward(const void* fmap1, const void* fmap2, int dtype, int b, int n1, int n2,
+                                    int c, int h, int w, int h2, int w2, const float* coords,
+                                    const int64_t* ii, const int64_t* jj, int m, const float* grad,
+                                    int radius, float scale, void* fmap1_grad, void* fmap2_grad,
+                                    int32_t* info, void* workspace, size_t workspace_bytes,
+                                    hs2_stream_t stream) {
+  using namespace hs2;
+  int rc = ac_check("altcorr_backward", b, n1, n2, c, h, w, h2, w2, m, radius);
+  if (rc) return rc;
+  size_t need = 0;
+  hs2_altcorr_backward_workspace_size(dtype, b, n1, n2, c, h, w, h2, w2, &need);
+  if (need > 0 && (workspace == nullptr || workspace_bytes < need)) {
+    set_error("altcorr_backward: workspace of %zu bytes required", need);
+    return HS2_ERR_WORKSPACE;
+  }
+  if ((rc = bind_device(fmap1_grad))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (dtype) {
+    case HS2_F32:
+      return ac_bwd<float>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, grad, radius, scale,
+                           fmap1_grad, fmap2_grad, info, workspace, s);
+    case HS2_F16:
+      return ac_bwd<__half>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, grad, radius, scale,
+                            fmap1_grad, fmap2_grad, info, workspace, s);
+    case HS2_BF16:
+      return ac_bwd<__nv_bfloat16>(fmap1, fmap2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, grad, radius,
+                                   scale, fmap1_grad, fmap2_grad, info, workspace, s);
+  }
+  set_error("altcorr_backward: unsupported dtype %d (f32, f16, bf16)", dtype);
+  return HS2_ERR_DTYPE;
+}

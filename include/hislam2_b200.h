@@ -1,0 +1,176 @@
+/*
+ * hislam2_b200 — C ABI of the B200 (sm_100a) dense-BA + correlation operators.
+ *
+ * Each entry point replaces one operator of HI-SLAM2's compiled extension
+ * `droid_backends` (bound in src/droid.cpp:325-341 of the reference).  The
+ * signatures take plain device pointers, sizes and a CUDA stream; nothing here
+ * depends on PyTorch.  All tensors are dense, row-major ("contiguous") and live
+ * on the device that owns them; work is enqueued on `stream` and the calls do
+ * not synchronise unless stated.
+ *
+ * Return value: HS2_OK or an HS2_ERR_* code; hs2_last_error() gives the message
+ * (thread-local).  Errors that depend on device-resident data (an edge index out
+ * of range, a wrong eta height) are reported in the `info` words, which the
+ * kernels write and the caller reads after the stream has drained.
+ */
+#ifndef HISLAM2_B200_H_
+#define HISLAM2_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* hs2_stream_t; /* == cudaStream_t; NULL = legacy default stream */
+
+enum hs2_status {
+  HS2_OK = 0,
+  HS2_ERR_INVALID = 1,   /* bad sizes / arguments detected on the host */
+  HS2_ERR_CUDA = 2,      /* a CUDA runtime call or launch failed */
+  HS2_ERR_WORKSPACE = 3, /* workspace pointer missing or too small */
+  HS2_ERR_DTYPE = 4      /* unsupported element type */
+};
+
+enum hs2_dtype { HS2_F32 = 0, HS2_F16 = 1, HS2_BF16 = 2, HS2_F64 = 3 };
+
+/* Bits of info[0] written on the device. */
+enum hs2_device_error {
+  HS2_DEV_BAD_INDEX = 1, /* an edge index lies outside the pose/disparity buffers or >= t1 */
+  HS2_DEV_BAD_ETA = 2    /* eta has neither M nor 1 rows (M = #distinct depth frames) */
+};
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* hs2_last_error(void);
+/* ABI version, (major << 16) | minor. */
+int hs2_version(void);
+
+/* ---------------------------------------------------------------------------
+ * frame_distance  (reference: src/droid.cpp:200-216, src/droid_kernels.cu:860-994,2047-2069)
+ *   poses [num_poses,7] f32, disps [num_disps,ht,wd] f32, intrinsics [4] f32,
+ *   ii/jj [num_edges] int64  ->  dist [num_edges] f32.
+ *   info: int32[1] on the device; info[0] |= HS2_DEV_BAD_INDEX for an edge whose
+ *   index is outside the buffers (its dist is then 1000).
+ */
+int hs2_frame_distance(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps,
+                       int ht, int wd, const float* intrinsics, const int64_t* ii, const int64_t* jj,
+                       int64_t num_edges, float beta, float* dist, int32_t* info, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * corr_index_forward  (reference: src/droid.cpp:254-264, src/correlation_kernels.cu:19-70,127-154)
+ *   volume [n,h1,w1,h2,w2] of `dtype`, coords [n,2,h1,w1] f32
+ *   -> corr [n,2r+1,2r+1,h1,w1] of `dtype` (dim 1 along x, dim 2 along y).
+ *   Every element of corr is written (no pre-zeroing needed).
+ */
+int hs2_corr_index_forward(const void* volume, int dtype, int64_t n, int h1, int w1, int h2, int w2,
+                           const float* coords, int radius, void* corr, hs2_stream_t stream);
+
+/* corr_index_backward  (reference: src/droid.cpp:266-275, src/correlation_kernels.cu:73-124,156-184)
+ *   coords [n,2,h1,w1] f32, corr_grad [n,2r+1,2r+1,h1,w1] of `dtype`
+ *   -> volume_grad [n,h1,w1,h2,w2] of `dtype`, fully written (zeros outside the windows).
+ */
+int hs2_corr_index_backward(const float* coords, const void* corr_grad, int dtype, int64_t n, int h1,
+                            int w1, int h2, int w2, int radius, void* volume_grad, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * altcorr_forward  (reference: src/droid.cpp:277-289, src/altcorr_kernel.cu:25-75,132-172)
+ *   fmap1 [b,n1,c,h,w], fmap2 [b,n2,c,h2,w2] of `dtype`, coords [b,m,2,h,w] f32,
+ *   ii/jj [m] int64 (frame of fmap1 / fmap2 for each of the m correlations)
+ *   -> corr [b,m,2r+1,2r+1,h,w] of `dtype`, dim 2 along x and dim 3 along y,
+ *   values (f1/4).(f2/4) bilinearly sampled.  Written densely (contiguous).
+ *   info: int32[1]; HS2_DEV_BAD_INDEX for an ii/jj outside [0,n1)/[0,n2) (that
+ *   correlation is then all zeros).
+ */
+int hs2_altcorr_forward(const void* fmap1, const void* fmap2, int dtype, int b, int n1, int n2, int c,
+                        int h, int w, int h2, int w2, const float* coords, const int64_t* ii,
+                        const int64_t* jj, int m, int radius, void* corr, int32_t* info,
+                        hs2_stream_t stream);
+
+/* altcorr_backward  (reference: src/droid.cpp:291-305, src/altcorr_kernel.cu:79-129,175-225;
+ *   effective positional order as called from hislam2/modules/corr.py:86)
+ *   grad [b,m,2r+1,2r+1,h,w] f32 (same layout as the forward output).
+ *   -> fmap1_grad [b,n1,c,h,w], fmap2_grad [b,n2,c,h2,w2] of `dtype`, fully written.
+ *   `scale` multiplies every product: 1 reproduces the reference operator (which
+ *   leaves out the forward's 1/16), 1/16 gives the exact adjoint of the forward.
+ *   workspace: f32 accumulators, hs2_altcorr_backward_workspace_size() bytes
+ *   (0 when dtype is f32).
+ */
+int hs2_altcorr_backward_workspace_size(int dtype, int b, int n1, int n2, int c, int h, int w, int h2,
+                                        int w2, size_t* bytes);
+int hs2_altcorr_backward(const void* fmap1, const void* fmap2, int dtype, int b, int n1, int n2, int c,
+                         int h, int w, int h2, int w2, const float* coords, const int64_t* ii,
+                         const int64_t* jj, int m, const float* grad, int radius, float scale,
+                         void* fmap1_grad, void* fmap2_grad, int32_t* info, void* workspace,
+                         size_t workspace_bytes, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * ba  (reference: src/droid.cpp:141-168, src/droid_kernels.cu:1820-1937)
+ *   Runs `iterations` damped Gauss-Newton steps over the poses [t0,t1) and the
+ *   disparity maps of every frame in unique(cat(arange(t0,t1), ii)), updating
+ *   `poses` [num_poses,7] and `disps` [num_disps,ht,wd] IN PLACE.
+ *   intrinsics [4] f32 (one pinhole camera), targets/weights [num_edges,2,ht,wd] f32,
+ *   eta [eta_rows,ht,wd] f32 with eta_rows == M or 1, ii/jj [num_edges] int64,
+ *   every ii/jj in [0, min(num_poses,num_disps)) and < t1.
+ *   Outputs of the last iteration: dx [t1-t0,6] f32 and, unless motion_only,
+ *   dz [M,ht*wd] f32 (dz must hold dz_rows >= M rows; M <= min(num_poses, t1-t0+num_edges)).
+ *   info: int32[4] on the device: [0] HS2_DEV_* bits, [1] M, [2] number of
+ *   iterations whose Cholesky factorisation failed (their dx is 0, as in the
+ *   reference), [3] reserved.  When info[0] != 0 nothing was modified.
+ *   workspace: hs2_ba_workspace_size() bytes, 256-byte aligned.
+ *   No host synchronisation; safe to capture in a CUDA graph.
+ */
+int hs2_ba_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd, int64_t num_edges,
+                          int t0, int t1, int motion_only, size_t* bytes);
+int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num_disps, int ht, int wd,
+           const float* intrinsics, const float* targets, const float* weights, const float* eta,
+           int64_t eta_rows, const int64_t* ii, const int64_t* jj, int64_t num_edges, int t0, int t1,
+           int iterations, float lm, float ep, int motion_only, float* dx, float* dz, int64_t dz_rows,
+           int32_t* info, void* workspace, size_t workspace_bytes, hs2_stream_t stream);
+
+/* Key generation of ba alone, for parity checks of the integer keys
+ * (reference: src/droid_kernels.cu:1841-1849 unique/inverse, :1712-1740 schur rows).
+ *   kx [min(num_poses,t1-t0+num_edges)] int32: sorted distinct frames of cat(arange(t0,t1), ii);
+ *   kk_exp [t1-t0+num_edges] int32: inverse index of each row of cat(arange(t0,t1), ii);
+ *   rows_ptr [num_rows_cap+1] / rows [t1-t0+num_edges] int32: per depth slot k, the rows
+ *   n (0..t1-t0+num_edges) whose pose jj_exp[n] lies in [t0,t1), in increasing n.
+ *   info as for hs2_ba.  Uses the same workspace as hs2_ba.
+ */
+int hs2_ba_keys(int64_t num_poses, int64_t num_disps, int ht, int wd, const int64_t* ii,
+                const int64_t* jj, int64_t num_edges, int t0, int t1, int32_t* kx, int32_t* kk_exp,
+                int32_t* rows_ptr, int32_t* rows, int32_t* info, void* workspace,
+                size_t workspace_bytes, hs2_stream_t stream);
+
+/* The reduced camera system of one linearisation, for block-level parity checks
+ * (reference: the matrix (A - S) and vector (A.b - S.b) handed to
+ * SparseBlock::solve at src/droid_kernels.cu:1909, before damping).
+ *   A_out [6(t1-t0), 6(t1-t0)] f64 row-major (full symmetric), b_out [6(t1-t0)] f64;
+ *   motion_only gives the pose block A alone (src/droid_kernels.cu:1878-1898).
+ *   Arguments otherwise as for hs2_ba; poses and disps are not modified.
+ */
+int hs2_ba_reduced_system(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps,
+                          int ht, int wd, const float* intrinsics, const float* targets,
+                          const float* weights, const float* eta, int64_t eta_rows, const int64_t* ii,
+                          const int64_t* jj, int64_t num_edges, int t0, int t1, int motion_only,
+                          double* A_out, double* b_out, int32_t* info, void* workspace,
+                          size_t workspace_bytes, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Measurement support (no counterpart in the reference, which has no profiler).
+ * hs2_profile_enable(1) brackets every kernel launch of this library with CUDA
+ * events on its stream; hs2_profile_report() waits for them and writes one line
+ * per kernel, "<name> <launches> <total_ms>", into buf (returns the text length;
+ * reset != 0 clears the record).  hs2_measure_simt_peaks() times FP32 and FP64
+ * FMA chains on the current device (synchronous; allocates 8 bytes).
+ */
+void hs2_profile_enable(int on);
+/* Number of kernels this library has launched in this process. */
+long long hs2_launch_count(void);
+int hs2_profile_report(char* buf, size_t len, int reset);
+int hs2_measure_simt_peaks(double* fp32_tflops, double* fp64_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HISLAM2_B200_H_ */

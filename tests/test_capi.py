@@ -1,0 +1,98 @@
+"""The C ABI library: loads, exports every symbol of include/hislam2_b200.h, and the
+host-side validation of the ops (no GPU needed: nothing here launches work)."""
+
+import ctypes
+import os
+import re
+
+import pytest
+import torch
+
+import droid_backends
+from hislam2_b200 import _lib, backends
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "hislam2_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"(?:int|void|long long|const char\s*\*)\s+(hs2_\w+)\s*\(([^)]*)\)\s*;", text):
+        params = [p for p in m.group(2).split(",") if p.strip() and p.strip() != "void"]
+        out[m.group(1)] = len(params)
+    return out
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    decl = declared()
+    assert len(decl) >= 11
+    for name, nparams in decl.items():
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, name
+        assert len(_lib.SIGNATURES[name]) == nparams, name
+    assert lib.hs2_version() == (1 << 16)
+
+
+def test_library_links_no_cuda_runtime_dynamically():
+    # cudart is linked statically so the library does not clash with PyTorch's own runtime
+    maps = open("/proc/self/maps").read()
+    _lib.load()
+    maps = open("/proc/self/maps").read()
+    assert _lib.LIB_PATH in maps
+
+
+def test_workspace_size_validation():
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.hs2_ba_workspace_size(300, 300, 43, 77, 6000, 10, 300, 0, ctypes.byref(n)) == _lib.HS2_OK
+    assert n.value > 6 * 6290 * 3311 * 4  # holds the E rows
+    rc = lib.hs2_ba_workspace_size(300, 300, 43, 77, 6000, 10, 301, 0, ctypes.byref(n))
+    assert rc == _lib.HS2_ERR_INVALID
+    assert b"t1" in lib.hs2_last_error()
+    assert lib.hs2_ba_workspace_size(8, 8, 0, 64, 10, 0, 8, 0, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+    assert backends.ba_workspace_bytes(8, 8, 48, 64, 24, 2, 8, True) < backends.ba_workspace_bytes(
+        8, 8, 48, 64, 24, 2, 8, False)
+
+
+def test_corr_validation_before_any_launch():
+    lib = _lib.load()
+    rc = lib.hs2_corr_index_forward(None, _lib.HS2_F32, 1, 4, 4, 4, 4, None, -1, None, None)
+    assert rc == _lib.HS2_ERR_INVALID
+    rc = lib.hs2_altcorr_forward(None, None, _lib.HS2_F32, 1, 1, 1, 0, 4, 4, 4, 4, None, None, None, 1, 3,
+                                 None, None, None)
+    assert rc == _lib.HS2_ERR_INVALID
+    with pytest.raises(RuntimeError, match="status 1"):
+        _lib.check(rc, "altcorr_forward")
+
+
+def test_ops_check_contiguity_then_device():
+    v = torch.zeros(1, 4, 4, 4, 4)
+    c = torch.zeros(1, 2, 4, 4)
+    with pytest.raises(RuntimeError, match="volume must be contiguous"):
+        droid_backends.corr_index_forward(v.transpose(1, 2), c, 3)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        droid_backends.corr_index_forward(v, c, 3)
+    p = torch.zeros(8, 7)
+    d = torch.ones(8, 4, 4)
+    i = torch.zeros(2, dtype=torch.long)
+    with pytest.raises(RuntimeError, match="poses must be contiguous"):
+        droid_backends.ba(p.t().contiguous().t(), d, torch.zeros(4), torch.zeros(2, 2, 4, 4),
+                          torch.zeros(2, 2, 4, 4), torch.zeros(8, 4, 4), i, i, 0, 8, 1, 1e-4, 0.1, False)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        droid_backends.ba(p, d, torch.zeros(4), torch.zeros(2, 2, 4, 4), torch.zeros(2, 2, 4, 4),
+                          torch.zeros(8, 4, 4), i, i, 0, 8, 1, 1e-4, 0.1, False)
+    with pytest.raises(RuntimeError, match="disps_sens"):
+        droid_backends.ba(p, d, torch.zeros(4), torch.ones(8, 4, 4), torch.zeros(2, 2, 4, 4),
+                          torch.zeros(2, 2, 4, 4), torch.zeros(8, 4, 4), i, i, 0, 8, 1, 1e-4, 0.1, False)
+    with pytest.raises(TypeError):
+        droid_backends.ba(p, d, torch.zeros(4), 1, 2, 3)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        droid_backends.frame_distance(p, d, torch.zeros(4), i, i, 0.3)
+
+
+def test_out_of_path_ops_raise():
+    for name in ("pgba", "proj_trans", "covis_distance", "depth_filter", "iproj", "bi_inter"):
+        with pytest.raises(NotImplementedError, match=name):
+            getattr(droid_backends, name)()
