@@ -87,7 +87,8 @@ def test_reduced_system_matches_oracle(cuda, case, motion_only):
     Ao, bo = oracle_reduced_system(p, motion_only)
     assert rel(np64(A), Ao) < RTOL, rel(np64(A), Ao)
     assert rel(np64(b), bo) < RTOL, rel(np64(b), bo)
-    assert torch.equal(A, A.t())
+    # symmetric up to the order of the FP64 atomic sums
+    assert rel(np64(A), np64(A.t())) < 1e-12
 
 
 @pytest.mark.parametrize("case", list(CASES))
@@ -97,9 +98,12 @@ def test_ba_matches_oracle(cuda, case):
     r = run_oracle(p)
     assert rel(np64(poses), r.poses) < RTOL, rel(np64(poses), r.poses)
     assert rel(np64(disps), r.disps) < RTOL, rel(np64(disps), r.disps)
-    assert rel(np64(dz), r.dz) < 1e-3, rel(np64(dz), r.dz)
-    assert rel(np64(dx), r.dx) < 1e-3, rel(np64(dx), r.dx)
     assert dz.shape == (len(r.kx), p["disps"].shape[1] * p["disps"].shape[2])
+    # the step of the first iteration (later ones shrink towards the FP32 noise floor)
+    poses, disps, dx, dz = run_gpu(p, cuda, iters=1)
+    r = run_oracle(p, iters=1)
+    assert rel(np64(dx), r.dx) < 1e-4, rel(np64(dx), r.dx)
+    assert rel(np64(dz), r.dz) < 1e-4, rel(np64(dz), r.dz)
 
 
 def test_motion_only_matches_oracle(cuda):
@@ -109,7 +113,9 @@ def test_motion_only_matches_oracle(cuda):
     assert dz is None
     assert torch.equal(disps.cpu(), p["disps"])
     assert rel(np64(poses), r.poses) < RTOL
-    assert rel(np64(dx), r.dx) < 1e-3
+    poses, disps, dx, dz = run_gpu(p, cuda, iters=1, motion_only=True)
+    r = run_oracle(p, iters=1, motion_only=True)
+    assert rel(np64(dx), r.dx) < 1e-4
 
 
 @pytest.mark.parametrize("case", ["frontend", "backend40"])
@@ -129,8 +135,9 @@ def test_keys_bit_exact(cuda, case):
 
 def test_edge_cases_match_oracle(cuda):
     base = CASES["frontend_small"]()
-    # (a) no edges at all
+    # (a) no edges at all: the depth frames are the window frames alone
     p = dict(base)
+    p["eta"] = base["eta"][base["t0"]:].contiguous()
     for k in ("ii", "jj"):
         p[k] = base[k][:0]
     for k in ("targets", "weights"):
@@ -206,7 +213,7 @@ def test_backend300_full_size_properties(cuda):
     # one step solves the damped reduced system it builds (FP64 both sides)
     A, b = backends.ba_reduced_system(q["poses"], q["disps"], q["intrinsics"], q["targets"], q["weights"],
                                       q["eta"], q["ii"], q["jj"], q["t0"], q["t1"])
-    assert torch.equal(A, A.t())
+    assert rel(np64(A), np64(A.t())) < 1e-12
     Ad = A.clone()
     Ad.diagonal().add_(p["ep"] + p["lm"] * A.diagonal())
     x_ref = torch.linalg.solve(Ad, b)
