@@ -14,6 +14,7 @@ HS2_OK, HS2_ERR_INVALID, HS2_ERR_CUDA, HS2_ERR_WORKSPACE, HS2_ERR_DTYPE = range(
 HS2_F32, HS2_F16, HS2_BF16, HS2_F64 = range(4)
 HS2_DEV_BAD_INDEX = 1
 HS2_DEV_BAD_ETA = 2
+HS2_DEV_TIMEOUT = 4
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int

@@ -49,6 +49,8 @@ def _raise_device_errors(bits, op):
         raise RuntimeError("%s: an edge index is out of range (ii/jj outside the buffers or >= t1)" % op)
     if bits & _lib.HS2_DEV_BAD_ETA:
         raise RuntimeError("%s: eta must have M or 1 rows (M = number of distinct depth frames)" % op)
+    if bits & _lib.HS2_DEV_TIMEOUT:
+        raise RuntimeError("%s: a bounded in-kernel wait timed out; the results are not valid" % op)
 
 
 # --------------------------------------------------------------------------- ba

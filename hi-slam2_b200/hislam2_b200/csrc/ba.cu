@@ -36,16 +36,13 @@ constexpr int kLinThreads = 128;
 constexpr int kLinPPT = 4;                          // pixels per thread
 constexpr int kLinChunk = kLinThreads * kLinPPT;    // pixels per CTA
 constexpr int kSchurTP = 32;                        // pixels per smem stage
-constexpr int kSchurRows = 96;                      // 16 blocks of 6 rows
-constexpr int kSchurLd = 97;                        // padded smem row stride
-constexpr int kCholSmallN = 160;                    // single-CTA Cholesky limit
 constexpr int kNB = 64;                             // blocked Cholesky tile
 constexpr int kEtab = 48;                           // floats per edge in the edge table
 
 // ------------------------------------------------------------ workspace ---
 struct BaLayout {
   size_t flag, slot, kx, gptr, gedge, cursor, rptr, rrow, rpose, sptr, srow, spose;
-  size_t etab, etab64, hedge, erows, qbuf, wbuf, A, b, x, chol_fail, total;
+  size_t etab, etab64, hedge, erows, qbuf, wbuf, A, b, x, chol_fail, L11, dinv, ychol, ctl, total;
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -79,6 +76,10 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
   L.b = take(sizeof(double) * (size_t)(n + 1));
   L.x = take(sizeof(double) * (size_t)(n + 1));
   L.chol_fail = take(sizeof(int) * 4);
+  L.L11 = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB * kNB);
+  L.dinv = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB);
+  L.ychol = take(sizeof(double) * (size_t)(n + 1));
+  L.ctl = take(sizeof(unsigned) * 4);
   L.total = o;
   return L;
 }
@@ -469,14 +470,53 @@ __global__ void ba_assemble_kernel(const int64_t* __restrict__ ii, const int64_t
     }
   }
   if (j < 0) return;
+  // only the lower block triangle of the system is kept (the factorisation reads nothing else)
   for (int r = 0; r < 6; ++r)
     for (int c = 0; c < 6; ++c) {
-      atomicAdd(&A[(i * 6 + r) * n + j * 6 + c], Hij[r][c]);
-      atomicAdd(&A[(j * 6 + c) * n + i * 6 + r], Hij[r][c]);
+      if (i > j) atomicAdd(&A[(i * 6 + r) * n + j * 6 + c], Hij[r][c]);
+      else if (j > i) atomicAdd(&A[(j * 6 + c) * n + i * 6 + r], Hij[r][c]);
+      else atomicAdd(&A[(i * 6 + r) * n + i * 6 + c], Hij[r][c] + Hij[c][r]);
     }
 }
 
 // ---------------------------------------------------------------- schur ---
+// Per (depth frame k, pixel chunk): S_ab = sum_p Q E_a E_b^T for every pair of the
+// frame's Schur rows a <= b (6x6 blocks) and v_a = sum_p Q w E_a.  Rows are
+// processed in tiles of kSchurTB blocks; a CTA thread owns up to two items (a
+// block pair or a w pair) and keeps their 36 sums in registers while the rows'
+// values for 32 pixels at a time sit in shared memory.  Results go to the lower
+// triangle of the FP64 reduced camera system (all that the factorisation reads):
+// S_ab lands on block (pose_a, pose_b) when pose_a > pose_b and transposed on
+// (pose_b, pose_a) otherwise.
+constexpr int kSchurTB = 22;                 // row blocks per tile
+constexpr int kSchurTR = 6 * kSchurTB;       // rows per tile
+constexpr int kSchurItems = 2;               // items per thread
+
+__device__ __forceinline__ void schur_scatter_block(double* A, int64_t n, int pa, int pb, bool same_row,
+                                                    const float (&acc)[36]) {
+  if (pa > pb) {
+#pragma unroll
+    for (int x = 0; x < 6; ++x)
+#pragma unroll
+      for (int y = 0; y < 6; ++y) atomicAdd(&A[(pa * 6 + x) * n + pb * 6 + y], -(double)acc[x * 6 + y]);
+  } else if (pa < pb) {
+#pragma unroll
+    for (int x = 0; x < 6; ++x)
+#pragma unroll
+      for (int y = 0; y < 6; ++y) atomicAdd(&A[(pb * 6 + y) * n + pa * 6 + x], -(double)acc[x * 6 + y]);
+  } else {
+    // same pose: S_ab (+ S_ab^T for two different rows) on the diagonal block
+#pragma unroll
+    for (int x = 0; x < 6; ++x)
+#pragma unroll
+      for (int y = 0; y < 6; ++y) {
+        double v = -(double)acc[x * 6 + y];
+        if (!same_row) v -= (double)acc[y * 6 + x];
+        atomicAdd(&A[(pa * 6 + x) * n + pa * 6 + y], v);
+      }
+  }
+}
+
 __global__ void __launch_bounds__(256)
 ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, const int32_t* __restrict__ info) {
   if (info[0]) return;
@@ -485,364 +525,403 @@ ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, const int32_t* __restrict__ 
   const int r0 = w.sptr[s];
   const int nr = w.sptr[s + 1] - r0;
   if (nr == 0) return;
-  const int* srow = w.srow + r0;
-  const int* spose = w.spose + r0;
-  const int nblk = nr + 1;                 // + the w column block
-  const int ntile = (nblk + 15) / 16;
   const int c0 = blockIdx.y * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int* srow = w.srow + r0;
+  const int* spose = w.spose + r0;
   const int64_t n = 6 * (int64_t)P;
   const float* Q = w.qbuf + (int64_t)s * HW;
   const float* W = w.wbuf + (int64_t)s * HW;
 
-  __shared__ float As[kSchurTP * kSchurLd];
-  __shared__ float Bs[kSchurTP * kSchurLd];
+  __shared__ float Fa[kSchurTP][kSchurTR + 2];   // Q-scaled rows of tile mt
+  __shared__ float Fb[kSchurTP][kSchurTR + 2];   // rows of tile nt
+  __shared__ float Ws[kSchurTP];
 
+  const int ntile = (nr + kSchurTB - 1) / kSchurTB;
   for (int mt = 0; mt < ntile; ++mt) {
     for (int nt = mt; nt < ntile; ++nt) {
-      float acc[6][6];
+      const int na = min(kSchurTB, nr - mt * kSchurTB);
+      const int nb = min(kSchurTB, nr - nt * kSchurTB);
+      const bool diag = mt == nt;
+      const int npairs = diag ? na * (na + 1) / 2 : na * nb;
+      const int nitems = npairs + (diag ? na : 0);
+      int ia[kSchurItems], ib[kSchurItems];   // ib == -1: w pair
+      bool live[kSchurItems];
 #pragma unroll
-      for (int a = 0; a < 6; ++a)
+      for (int q = 0; q < kSchurItems; ++q) {
+        const int it = threadIdx.x + q * 256;
+        live[q] = it < nitems;
+        ia[q] = 0;
+        ib[q] = -1;
+        if (it < npairs) {
+          if (diag) {
+            // it -> (a, b) with a <= b, row-major over the upper triangle
+            int a = 0, rem = it;
+            while (rem >= na - a) { rem -= na - a; ++a; }
+            ia[q] = a;
+            ib[q] = a + rem;
+          } else {
+            ia[q] = it / nb;
+            ib[q] = it - (it / nb) * nb;
+          }
+        } else if (it < nitems) {
+          ia[q] = it - npairs;
+        }
+      }
+      float acc[kSchurItems][36];
 #pragma unroll
-        for (int b = 0; b < 6; ++b) acc[a][b] = 0.f;
+      for (int q = 0; q < kSchurItems; ++q)
+#pragma unroll
+        for (int k = 0; k < 36; ++k) acc[q][k] = 0.f;
 
       for (int p0 = c0; p0 < c1; p0 += kSchurTP) {
-        for (int idx = threadIdx.x; idx < kSchurRows * kSchurTP; idx += 256) {
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kSchurTR * kSchurTP; idx += 256) {
           const int row = idx / kSchurTP;
           const int pp = idx - row * kSchurTP;
           const int p = p0 + pp;
           const int blk = row / 6, d = row - (row / 6) * 6;
           float va = 0.f, vb = 0.f;
           if (p < c1) {
-            const int ba = mt * 16 + blk;
-            if (ba < nr) va = w.erows[((int64_t)srow[ba] * 6 + d) * HW + p] * Q[p];
-            const int bb = nt * 16 + blk;
-            if (bb < nr) vb = w.erows[((int64_t)srow[bb] * 6 + d) * HW + p];
-            else if (bb == nr && d == 0) vb = W[p];
+            if (blk < na) va = w.erows[((int64_t)srow[mt * kSchurTB + blk] * 6 + d) * HW + p] * Q[p];
+            if (blk < nb) vb = w.erows[((int64_t)srow[nt * kSchurTB + blk] * 6 + d) * HW + p];
           }
-          As[pp * kSchurLd + row] = va;
-          Bs[pp * kSchurLd + row] = vb;
+          Fa[pp][row] = va;
+          Fb[pp][row] = vb;
+        }
+        if (threadIdx.x < kSchurTP) {
+          const int p = p0 + threadIdx.x;
+          Ws[threadIdx.x] = p < c1 ? W[p] : 0.f;
         }
         __syncthreads();
-#pragma unroll 4
+#pragma unroll 2
         for (int pp = 0; pp < kSchurTP; ++pp) {
-          float a[6], b[6];
 #pragma unroll
-          for (int k = 0; k < 6; ++k) {
-            a[k] = As[pp * kSchurLd + ty * 6 + k];
-            b[k] = Bs[pp * kSchurLd + tx * 6 + k];
+          for (int q = 0; q < kSchurItems; ++q) {
+            if (!live[q]) continue;
+            float av[6];
+#pragma unroll
+            for (int x = 0; x < 6; ++x) av[x] = Fa[pp][ia[q] * 6 + x];
+            if (ib[q] >= 0) {
+              float bv[6];
+#pragma unroll
+              for (int y = 0; y < 6; ++y) bv[y] = Fb[pp][ib[q] * 6 + y];
+#pragma unroll
+              for (int x = 0; x < 6; ++x)
+#pragma unroll
+                for (int y = 0; y < 6; ++y) acc[q][x * 6 + y] += av[x] * bv[y];
+            } else {
+              const float wv = Ws[pp];
+#pragma unroll
+              for (int x = 0; x < 6; ++x) acc[q][x] += av[x] * wv;
+            }
           }
-#pragma unroll
-          for (int x = 0; x < 6; ++x)
-#pragma unroll
-            for (int y = 0; y < 6; ++y) acc[x][y] += a[x] * b[y];
         }
-        __syncthreads();
       }
-
-      const int ra = mt * 16 + ty, rb = nt * 16 + tx;
-      if (ra >= nr) continue;
-      const int pa = spose[ra];
-      if (rb < nr) {
-        if (mt == nt && ty > tx) continue;
-        const int pb = spose[rb];
 #pragma unroll
-        for (int x = 0; x < 6; ++x)
+      for (int q = 0; q < kSchurItems; ++q) {
+        if (!live[q]) continue;
+        const int ra = mt * kSchurTB + ia[q];
+        const int pa = spose[ra];
+        if (ib[q] >= 0) {
+          const int rb = nt * kSchurTB + ib[q];
+          schur_scatter_block(w.A, n, pa, spose[rb], ra == rb, acc[q]);
+        } else {
 #pragma unroll
-          for (int y = 0; y < 6; ++y) {
-            const double v = -(double)acc[x][y];
-            atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], v);
-            if (ra != rb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], v);
-          }
-      } else if (rb == nr) {
-#pragma unroll
-        for (int x = 0; x < 6; ++x) atomicAdd(&w.b[pa * 6 + x], -(double)acc[x][0]);
+          for (int x = 0; x < 6; ++x) atomicAdd(&w.b[pa * 6 + x], -(double)acc[q][x]);
+        }
       }
     }
   }
+}
+
+// Mirrors the lower triangle of the reduced system into the upper one (diagnostics only).
+__global__ void ba_symmetrize_kernel(int n, double* __restrict__ A) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int i = (int)(idx / n), j = (int)(idx - (idx / n) * n);
+  if (j > i) A[idx] = A[(int64_t)j * n + i];
 }
 
 // ------------------------------------------------------------- cholesky ---
-// Single-CTA damped Cholesky + solve for n <= kCholSmallN, matrix in shared memory.
-__global__ void __launch_bounds__(512)
-ba_chol_small_kernel(int n, float lm, float ep, BaPtrs w, float* __restrict__ dx_out,
-                     int32_t* __restrict__ info) {
+// Damped FP64 Cholesky factorisation + solve of the reduced camera system in one
+// cooperative (persistent) launch.  Phases are separated by a grid barrier:
+//
+//   damping     diag += ep + lm*diag
+//   per 64-wide panel kb
+//     panel     every CTA owning a panel tile eliminates the 64 panel columns of
+//               [D; X | b] (D the diagonal block, redundantly in every such CTA;
+//               X its 64-row tile below; b the right-hand side), register-resident
+//               16x16 threads x 4x4 elements, one __syncthreads per column.  The tile
+//               of D writes L11 and y = L11^-1 b1; the others write L21 and b2 - L21 y1.
+//     syrk      trailing update A22 -= L21 L21^T on the lower 64x64 tiles
+//   backward    per panel from the last: x_kb = L11^-T y_kb, then y_c -= L[kb][c] . x_kb
+//               for every column c left of the panel
+//
+// A non-positive pivot (the matrix is not positive definite) is seen identically
+// by every CTA that factors the panel; the solution is then 0, as in the
+// reference's solver fallback.  Every spin of the grid barrier is bounded: on
+// timeout the kernel sets HS2_DEV_TIMEOUT and returns.
+constexpr int kCholThreads = 256;
+constexpr unsigned kBarrierSpins = 1u << 22;
+
+struct CholBuf {
+  double* L11;      // [nbk][64][64] factored diagonal blocks
+  double* dinv;     // [nbk][64] reciprocals of their diagonals
+  double* y;        // [n] forward-substituted right-hand side
+  unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed
+};
+
+__device__ __forceinline__ bool grid_barrier(unsigned* ctl, unsigned nblocks, int32_t* info) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen_p = ctl + 1;
+    const unsigned gen = *gen_p;
+    __threadfence();
+    const unsigned arrived = atomicAdd(ctl, 1u) + 1u;
+    int ok = 1;
+    if (arrived == nblocks) {
+      atomicExch(ctl, 0u);
+      __threadfence();
+      atomicAdd(ctl + 1, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*gen_p == gen) {
+        if (++spins > kBarrierSpins) {
+          ok = 0;
+          atomicOr(info, HS2_DEV_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kCholThreads, 1)
+ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __restrict__ dx_out,
+                   int32_t* __restrict__ info) {
   if (info[0]) return;
-  extern __shared__ double sm[];
-  double* Ms = sm;            // n*n
-  double* y = sm + n * n;     // n
-  __shared__ int fail;
-  if (threadIdx.x == 0) fail = 0;
-  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-    const int i = idx / n, j = idx - (idx / n) * n;
-    double v = w.A[idx];
-    if (i == j) v += ep + lm * v;
-    Ms[idx] = v;
-  }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = w.b[i];
-  __syncthreads();
-  for (int j = 0; j < n; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = Ms[j * n + j];
-      if (!(d > 0.0)) fail = 1;
-      else Ms[j * n + j] = sqrt(d);
-    }
-    __syncthreads();
-    if (fail) break;
-    const double piv = Ms[j * n + j];
-    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) Ms[i * n + j] /= piv;
-    __syncthreads();
-    const int m = n - j - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int i = j + 1 + idx / m, l = j + 1 + idx - (idx / m) * m;
-      if (l <= i) Ms[i * n + l] -= Ms[i * n + j] * Ms[l * n + j];
-    }
-    __syncthreads();
-  }
-  if (!fail && threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    // forward: L y = b
-    for (int j = 0; j < n; ++j) {
-      const double yj = y[j] / Ms[j * n + j];
-      __syncwarp();
-      if (lane == 0) y[j] = yj;
-      for (int i = j + 1 + lane; i < n; i += 32) y[i] -= Ms[i * n + j] * yj;
-      __syncwarp();
-    }
-    // backward: L^T x = y
-    for (int j = n - 1; j >= 0; --j) {
-      const double xj = y[j] / Ms[j * n + j];
-      __syncwarp();
-      if (lane == 0) y[j] = xj;
-      for (int i = lane; i < j; i += 32) y[i] -= Ms[j * n + i] * xj;
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double v = fail ? 0.0 : y[i];
-    w.x[i] = v;
-    dx_out[i] = (float)v;
-  }
-  if (threadIdx.x == 0 && fail) atomicAdd(&info[2], 1);
-}
+  extern __shared__ double csm[];
+  __shared__ double colD[2][kNB], colX[2][kNB], sbj[2], piv[2][4];
+  const unsigned G = gridDim.x;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int nbk = (n + kNB - 1) / kNB;
+  double* A = w.A;
+  double* bvec = w.b;
 
-// Blocked right-looking Cholesky for larger systems: damping, then per 64-wide
-// panel a diagonal factorisation (+ forward solve of b), a panel TRSM and a
-// trailing SYRK; then a blocked backward solve.  A failed pivot raises
-// chol_fail and every later step becomes a no-op; dx is then 0.
-__global__ void ba_chol_damp_kernel(int n, float lm, float ep, BaPtrs w) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
-    double* d = &w.A[(int64_t)i * n + i];
-    *d += ep + lm * *d;
+  for (int i = blockIdx.x * kCholThreads + tid; i < n; i += G * kCholThreads) {
+    double* d = &A[(int64_t)i * n + i];
+    *d += (double)ep + (double)lm * __ldcg(d);
   }
-  if (i == 0) w.chol_fail[0] = 0;
-}
+  if (!grid_barrier(cb.ctl, G, info)) return;
 
-__global__ void __launch_bounds__(256)
-ba_chol_diag_kernel(int n, int kb, BaPtrs w, const int32_t* __restrict__ info) {
-  if (info[0] || w.chol_fail[0]) return;
-  __shared__ double D[kNB][kNB + 1];
-  __shared__ double yb[kNB];
-  __shared__ int fail;
-  const int o = kb * kNB;
-  const int nb = min(kNB, n - o);
-  if (threadIdx.x == 0) fail = 0;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx / nb, j = idx - (idx / nb) * nb;
-    D[i][j] = w.A[(int64_t)(o + i) * n + o + j];
-  }
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) yb[i] = w.b[o + i];
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = D[j][j];
-      if (!(d > 0.0)) fail = 1;
-      else D[j][j] = sqrt(d);
-    }
-    __syncthreads();
-    if (fail) break;
-    const double piv = D[j][j];
-    for (int i = j + 1 + threadIdx.x; i < nb; i += blockDim.x) D[i][j] /= piv;
-    __syncthreads();
-    const int m = nb - j - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int i = j + 1 + idx / m, l = j + 1 + idx - (idx / m) * m;
-      if (l <= i) D[i][l] -= D[i][j] * D[l][j];
-    }
-    __syncthreads();
-  }
-  if (fail) {
-    if (threadIdx.x == 0) w.chol_fail[0] = 1;
-    return;
-  }
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (int j = 0; j < nb; ++j) {
-      const double yj = yb[j] / D[j][j];
-      __syncwarp();
-      if (lane == 0) yb[j] = yj;
-      for (int i = j + 1 + lane; i < nb; i += 32) yb[i] -= D[i][j] * yj;
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx / nb, j = idx - (idx / nb) * nb;
-    if (j <= i) w.A[(int64_t)(o + i) * n + o + j] = D[i][j];
-  }
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) w.b[o + i] = yb[i];
-}
-
-// rows below the diagonal block: X L11^T = A21, then b2 -= X y1
-__global__ void __launch_bounds__(256)
-ba_chol_trsm_kernel(int n, int kb, BaPtrs w, const int32_t* __restrict__ info) {
-  if (info[0] || w.chol_fail[0]) return;
-  extern __shared__ double trsm_sm[];
-  double (*Ls)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(trsm_sm);
-  double (*Xs)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(trsm_sm + kNB * (kNB + 1));
-  double* y1 = trsm_sm + 2 * kNB * (kNB + 1);
-  const int o = kb * kNB;
-  const int nb = min(kNB, n - o);
-  const int r0 = o + nb + blockIdx.x * kNB;
-  const int nr = min(kNB, n - r0);
-  if (nr <= 0) return;
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx / nb, j = idx - (idx / nb) * nb;
-    Ls[i][j] = j <= i ? w.A[(int64_t)(o + i) * n + o + j] : 0.0;
-  }
-  for (int idx = threadIdx.x; idx < nr * nb; idx += blockDim.x) {
-    const int i = idx / nb, j = idx - (idx / nb) * nb;
-    Xs[i][j] = w.A[(int64_t)(r0 + i) * n + o + j];
-  }
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) y1[i] = w.b[o + i];
-  __syncthreads();
-  // 4 threads per row; row-wise forward substitution over the columns
-  const int row = threadIdx.x >> 2, part = threadIdx.x & 3;
-  const unsigned grp = 0xFu << ((threadIdx.x & 31) & ~3);
-  if (row < nr) {
-    for (int j = 0; j < nb; ++j) {
-      double s = 0.0;
-      for (int i = part; i < j; i += 4) s += Xs[row][i] * Ls[j][i];
-      s += __shfl_xor_sync(grp, s, 1, 4);
-      s += __shfl_xor_sync(grp, s, 2, 4);
-      const double v = (Xs[row][j] - s) / Ls[j][j];
-      __syncwarp(grp);
-      if (part == 0) Xs[row][j] = v;
-      __syncwarp(grp);
-    }
-  } else {
-    // keep the shuffle groups of idle rows consistent
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < nr * nb; idx += blockDim.x) {
-    const int i = idx / nb, j = idx - (idx / nb) * nb;
-    w.A[(int64_t)(r0 + i) * n + o + j] = Xs[i][j];
-  }
-  for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-    double s = 0.0;
-    for (int j = 0; j < nb; ++j) s += Xs[i][j] * y1[j];
-    w.b[r0 + i] -= s;
-  }
-}
-
-// trailing update A22 -= L21 L21^T on the lower-triangular 64x64 tiles
-__global__ void __launch_bounds__(256)
-ba_chol_syrk_kernel(int n, int kb, BaPtrs w, const int32_t* __restrict__ info) {
-  if (info[0] || w.chol_fail[0]) return;
-  constexpr int KC = 32;
-  __shared__ double Ai[kNB][KC + 1];
-  __shared__ double Aj[kNB][KC + 1];
-  const int o = kb * kNB;
-  const int base = o + kNB;
-  // tile index -> (I, J) with I >= J
-  int t = blockIdx.x, I = 0;
-  while (t > I) { t -= I + 1; ++I; }
-  const int J = t;
-  const int ri = base + I * kNB, rj = base + J * kNB;
-  const int ni = min(kNB, n - ri), nj = min(kNB, n - rj);
-  if (ni <= 0 || nj <= 0) return;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int k0 = 0; k0 < kNB; k0 += KC) {
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kNB * KC; idx += blockDim.x) {
-      const int a = idx / KC, k = idx - (idx / KC) * KC;
-      Ai[a][k] = a < ni ? w.A[(int64_t)(ri + a) * n + o + k0 + k] : 0.0;
-      Aj[a][k] = a < nj ? w.A[(int64_t)(rj + a) * n + o + k0 + k] : 0.0;
-    }
-    __syncthreads();
-    for (int k = 0; k < KC; ++k) {
-      double xa[4], xb[4];
+  bool failed = false;
+  for (int kb = 0; kb < nbk && !failed; ++kb) {
+    const int o = kb * kNB;
+    const int nb = min(kNB, n - o);
+    const int rest = nbk - kb - 1;
+    // ---- panel
+    for (int t = blockIdx.x; t <= rest; t += G) {
+      const int r0 = o + nb + (t - 1) * kNB;
+      const int nr = t == 0 ? 0 : min(kNB, n - r0);
+      double d[4][4], x[4][4], bd[4], bx[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        xa[a] = Ai[ty + 16 * a][k];
-        xb[a] = Aj[tx + 16 * a][k];
+        const int i = ty * 4 + a;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int l = tx * 4 + c;
+          d[a][c] = (i < nb && l < nb) ? __ldcg(&A[(int64_t)(o + i) * n + o + l]) : 0.0;
+          x[a][c] = (i < nr && l < nb) ? __ldcg(&A[(int64_t)(r0 + i) * n + o + l]) : 0.0;
+        }
+        bd[a] = i < nb ? __ldcg(&bvec[o + i]) : 0.0;
+        bx[a] = i < nr ? __ldcg(&bvec[r0 + i]) : 0.0;
+      }
+      bool bad = false;
+      for (int j = 0; j < nb; ++j) {
+        const int p = j & 1;
+        const int cj = j & 3;
+        if (tx == (j >> 2)) {
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            // select column cj without dynamic register indexing
+            double vd = d[a][0], vx = x[a][0];
+            if (cj == 1) { vd = d[a][1]; vx = x[a][1]; }
+            if (cj == 2) { vd = d[a][2]; vx = x[a][2]; }
+            if (cj == 3) { vd = d[a][3]; vx = x[a][3]; }
+            colD[p][ty * 4 + a] = vd;
+            colX[p][ty * 4 + a] = vx;
+            if (ty == (j >> 2) && a == cj) {
+              // pivot owner: reciprocals once per column
+              const double sq = vd > 0.0 ? sqrt(vd) : 0.0;
+              const double sinv = vd > 0.0 ? 1.0 / sq : 0.0;
+              piv[p][0] = vd;
+              piv[p][1] = sinv * sinv;
+              piv[p][2] = sq;
+              piv[p][3] = sinv;
+            }
+          }
+        }
+        if (tx == 0 && ty == (j >> 2)) sbj[p] = cj == 0 ? bd[0] : cj == 1 ? bd[1] : cj == 2 ? bd[2] : bd[3];
+        __syncthreads();
+        if (!(piv[p][0] > 0.0)) {
+          bad = true;
+          break;
+        }
+        const double rinv = piv[p][1], sq = piv[p][2], sinv = piv[p][3];
+        const double bjr = sbj[p] * rinv;
+        double cl[4], ci[4], xi[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cl[c] = colD[p][tx * 4 + c] * rinv;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          ci[a] = colD[p][ty * 4 + a];
+          xi[a] = colX[p][ty * 4 + a];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int i = ty * 4 + a;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int l = tx * 4 + c;
+            if (l > j) {
+              if (i > j) d[a][c] -= ci[a] * cl[c];
+              x[a][c] -= xi[a] * cl[c];
+            } else if (l == j) {
+              d[a][c] = i > j ? d[a][c] * sinv : (i == j ? sq : d[a][c]);
+              x[a][c] *= sinv;
+            }
+          }
+          if (tx == 0) {
+            if (i > j) bd[a] -= ci[a] * bjr;
+            else if (i == j) bd[a] *= sinv;
+            bx[a] -= xi[a] * bjr;
+          }
+        }
+      }
+      if (bad) {
+        if (tid == 0) atomicExch(cb.ctl + 2, 1u);
+        break;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = ty * 4 + a;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int l = tx * 4 + c;
+          if (t == 0) {
+            cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? d[a][c] : 0.0;
+            if (l == i && i < nb) cb.dinv[(int64_t)kb * kNB + i] = 1.0 / d[a][c];
+          } else if (i < nr && l < nb) {
+            A[(int64_t)(r0 + i) * n + o + l] = x[a][c];
+          }
+        }
+        if (tx == 0) {
+          if (t == 0 && i < nb) cb.y[o + i] = bd[a];
+          if (t != 0 && i < nr) bvec[r0 + i] = bx[a];
+        }
+      }
+    }
+    if (!grid_barrier(cb.ctl, G, info)) return;
+    if (*(volatile unsigned*)(cb.ctl + 2)) {
+      failed = true;
+      break;
+    }
+    // ---- trailing update
+    const int ntiles = rest * (rest + 1) / 2;
+    double (*Ai)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm);
+    double (*Aj)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm + kNB * (kNB + 1));
+    for (int t = blockIdx.x; t < ntiles; t += G) {
+      int I = 0, tt = t;
+      while (tt > I) { tt -= I + 1; ++I; }
+      const int J = tt;
+      const int ri = o + kNB + I * kNB, rj = o + kNB + J * kNB;
+      const int ni = min(kNB, n - ri), nj = min(kNB, n - rj);
+      __syncthreads();
+      for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
+        const int a = idx >> 6, k = idx & 63;
+        Ai[a][k] = a < ni ? __ldcg(&A[(int64_t)(ri + a) * n + o + k]) : 0.0;
+        Aj[a][k] = a < nj ? __ldcg(&A[(int64_t)(rj + a) * n + o + k]) : 0.0;
+      }
+      __syncthreads();
+      double acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < kNB; ++k) {
+        double va[4], vb[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          va[a] = Ai[ty + 16 * a][k];
+          vb[a] = Aj[tx + 16 * a][k];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[a][c] += va[a] * vb[c];
       }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] += xa[a] * xb[b];
+        for (int c = 0; c < 4; ++c) {
+          const int i = ty + 16 * a, j = tx + 16 * c;
+          if (i < ni && j < nj && (I > J || j <= i)) {
+            double* dst = &A[(int64_t)(ri + i) * n + rj + j];
+            *dst = __ldcg(dst) - acc[a][c];
+          }
+        }
+    }
+    if (!grid_barrier(cb.ctl, G, info)) return;
+  }
+
+  if (!failed) {
+    double (*Ls)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm);
+    double* ys = csm + kNB * (kNB + 1);
+    for (int kb = nbk - 1; kb >= 0; --kb) {
+      const int o = kb * kNB;
+      const int nb = min(kNB, n - o);
+      __syncthreads();
+      for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
+        const int i = idx >> 6, l = idx & 63;
+        Ls[i][l] = __ldcg(&cb.L11[((int64_t)kb * kNB + i) * kNB + l]);
+      }
+      for (int i = tid; i < nb; i += kCholThreads) ys[i] = __ldcg(&cb.y[o + i]);
+      __syncthreads();
+      if (tid < 32) {
+        for (int j = nb - 1; j >= 0; --j) {
+          const double xj = ys[j] * __ldcg(&cb.dinv[(int64_t)kb * kNB + j]);
+          __syncwarp();
+          if (tid == 0) ys[j] = xj;
+          for (int i = tid; i < j; i += 32) ys[i] -= Ls[j][i] * xj;
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      if (blockIdx.x == 0)
+        for (int i = tid; i < nb; i += kCholThreads) w.x[o + i] = ys[i];
+      for (int c = blockIdx.x * kCholThreads + tid; c < o; c += G * kCholThreads) {
+        double s = 0.0;
+        for (int r = 0; r < nb; ++r) s += __ldcg(&A[(int64_t)(o + r) * n + c]) * ys[r];
+        cb.y[c] = __ldcg(&cb.y[c]) - s;
+      }
+      if (!grid_barrier(cb.ctl, G, info)) return;
     }
   }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 16 * b;
-      if (i < ni && j < nj && (I > J || j <= i)) w.A[(int64_t)(ri + i) * n + rj + j] -= acc[a][b];
-    }
-}
-
-// backward solve, diagonal block: x_kb = L11^-T y_kb
-__global__ void ba_chol_bdiag_kernel(int n, int kb, BaPtrs w, const int32_t* __restrict__ info) {
-  if (info[0] || w.chol_fail[0]) return;
-  __shared__ double yb[kNB];
-  const int o = kb * kNB;
-  const int nb = min(kNB, n - o);
-  const int lane = threadIdx.x;
-  for (int i = lane; i < nb; i += 32) yb[i] = w.b[o + i];
-  __syncwarp();
-  for (int j = nb - 1; j >= 0; --j) {
-    const double xj = yb[j] / w.A[(int64_t)(o + j) * n + o + j];
-    __syncwarp();
-    if (lane == 0) yb[j] = xj;
-    for (int i = lane; i < j; i += 32) yb[i] -= w.A[(int64_t)(o + j) * n + o + i] * xj;
-    __syncwarp();
-  }
-  for (int i = lane; i < nb; i += 32) w.b[o + i] = yb[i];
-}
-
-// backward solve, off-diagonal: y_J -= L[kb][J]^T x_kb for every block J < kb
-__global__ void __launch_bounds__(256)
-ba_chol_bupdate_kernel(int n, int kb, BaPtrs w, const int32_t* __restrict__ info) {
-  if (info[0] || w.chol_fail[0]) return;
-  const int o = kb * kNB;
-  const int nb = min(kNB, n - o);
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;  // column index < o
-  if (c >= o) return;
-  double s = 0.0;
-  for (int r = 0; r < nb; ++r) s += w.A[(int64_t)(o + r) * n + c] * w.b[o + r];
-  w.b[c] -= s;
-}
-
-__global__ void ba_chol_finish_kernel(int n, BaPtrs w, float* __restrict__ dx_out, int32_t* __restrict__ info) {
-  if (info[0]) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool fail = w.chol_fail[0] != 0;
-  if (i < n) {
-    const double v = fail ? 0.0 : w.b[i];
-    w.x[i] = v;
+  for (int i = blockIdx.x * kCholThreads + tid; i < n; i += G * kCholThreads) {
+    const double v = failed ? 0.0 : __ldcg(&w.x[i]);
+    if (failed) w.x[i] = 0.0;
     dx_out[i] = (float)v;
   }
-  if (i == 0 && fail) atomicAdd(&info[2], 1);
+  if (failed && blockIdx.x == 0 && tid == 0) atomicAdd(&info[2], 1);
 }
 
 // -------------------------------------------------------------- backsub ---
@@ -956,43 +1035,29 @@ static int run_keys(const BaProblem& pb, const int64_t* ii, const int64_t* jj, i
   return HS2_OK;
 }
 
-static int run_cholesky(int n, float lm, float ep, BaPtrs w, float* dx, int32_t* info, cudaStream_t s) {
+static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* dx, int32_t* info,
+                        cudaStream_t s) {
   if (n == 0) return HS2_OK;
   HS2_PROF("ba_cholesky", s);
-  if (n <= kCholSmallN) {
-    const size_t smem = sizeof(double) * ((size_t)n * n + n);
-    HS2_CUDA(cudaFuncSetAttribute(ba_chol_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ba_chol_small_kernel<<<1, 512, smem, s>>>(n, lm, ep, w, dx, info);
-    HS2_LAUNCH_CHECK("ba_chol_small_kernel");
-    return HS2_OK;
-  }
-  constexpr int kTrsmSmem = sizeof(double) * (2 * kNB * (kNB + 1) + kNB);
-  HS2_CUDA(cudaFuncSetAttribute(ba_chol_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsmSmem));
-  ba_chol_damp_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, lm, ep, w);
-  HS2_LAUNCH_CHECK("ba_chol_damp_kernel");
   const int nbk = (n + kNB - 1) / kNB;
-  for (int kb = 0; kb < nbk; ++kb) {
-    ba_chol_diag_kernel<<<1, 256, 0, s>>>(n, kb, w, info);
-    HS2_LAUNCH_CHECK("ba_chol_diag_kernel");
-    const int rest = nbk - kb - 1;
-    if (rest > 0) {
-      ba_chol_trsm_kernel<<<rest, 256, kTrsmSmem, s>>>(n, kb, w, info);
-      HS2_LAUNCH_CHECK("ba_chol_trsm_kernel");
-      ba_chol_syrk_kernel<<<rest * (rest + 1) / 2, 256, 0, s>>>(n, kb, w, info);
-      HS2_LAUNCH_CHECK("ba_chol_syrk_kernel");
-    }
+  const size_t smem = sizeof(double) * 2 * kNB * (kNB + 1);
+  static int grid_cap[64] = {0};
+  int dev = 0;
+  HS2_CUDA(cudaGetDevice(&dev));
+  if (dev >= 64) dev = 63;
+  if (grid_cap[dev] == 0) {
+    int sms = 0, occ = 0;
+    HS2_CUDA(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HS2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HS2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ba_cholesky_kernel, kCholThreads, smem));
+    grid_cap[dev] = std::max(1, std::min(occ, 1) * sms);
   }
-  for (int kb = nbk - 1; kb >= 0; --kb) {
-    ba_chol_bdiag_kernel<<<1, 32, 0, s>>>(n, kb, w, info);
-    HS2_LAUNCH_CHECK("ba_chol_bdiag_kernel");
-    if (kb > 0) {
-      const int cols = kb * kNB;
-      ba_chol_bupdate_kernel<<<(cols + 255) / 256, 256, 0, s>>>(n, kb, w, info);
-      HS2_LAUNCH_CHECK("ba_chol_bupdate_kernel");
-    }
-  }
-  ba_chol_finish_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, w, dx, info);
-  HS2_LAUNCH_CHECK("ba_chol_finish_kernel");
+  const int work = std::max(std::max(nbk, (nbk - 1) * nbk / 2), (n + kCholThreads - 1) / kCholThreads);
+  int G = std::max(1, std::min(grid_cap[dev], work));
+  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, 4 * sizeof(unsigned), s));
+  void* args[] = {&n, &lm, &ep, &w, &cb, &dx, &info};
+  HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_cholesky_kernel, dim3(G), dim3(kCholThreads), args, smem, s));
+  HS2_LAUNCH_CHECK("ba_cholesky_kernel");
   return HS2_OK;
 }
 
@@ -1004,8 +1069,9 @@ static BaLaunch ba_launch_shape(const BaProblem& p) {
   BaLaunch l;
   const int64_t S = std::min<int64_t>(p.K, (int64_t)p.P + p.E);
   l.nchunk = (p.HW + kLinChunk - 1) / kLinChunk;
-  // Schur split: enough CTAs to fill the GPU when there are few depth frames
-  l.schur_split = (int)std::max<int64_t>(1, std::min<int64_t>(8, (2 * kNumSMs + S - 1) / std::max<int64_t>(S, 1)));
+  // Schur split: about 8 waves of CTAs (2 resident per SM), chunks of >= 128 pixels
+  l.schur_split = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, p.HW / 128),
+                                                              (16 * kNumSMs + S - 1) / std::max<int64_t>(S, 1)));
   l.schur_chunk = (p.HW + l.schur_split - 1) / l.schur_split;
   l.schur_chunk = (l.schur_chunk + kSchurTP - 1) / kSchurTP * kSchurTP;
   l.schur_split = (p.HW + l.schur_chunk - 1) / l.schur_chunk;
@@ -1131,11 +1197,13 @@ extern "C" int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num
   const int64_t S = std::min<int64_t>(p.K, (int64_t)P + p.E);
   const BaLaunch l = ba_launch_shape(p);
   const int nchunk = l.nchunk;
+  char* wsb = static_cast<char*>(workspace);
+  CholBuf cb{(double*)(wsb + L.L11), (double*)(wsb + L.dinv), (double*)(wsb + L.ychol), (unsigned*)(wsb + L.ctl)};
 
   for (int it = 0; it < iterations; ++it) {
     if ((rc = build_system(p, l, poses, disps, intrinsics, targets, weights, eta, eta_rows, ii, jj, w, info, s)))
       return rc;
-    if ((rc = run_cholesky(n, lm, ep, w, dx, info, s))) return rc;
+    if ((rc = run_cholesky(n, lm, ep, w, cb, dx, info, s))) return rc;
     if (!p.motion_only && S > 0) {
       dim3 grid((unsigned)S, nchunk);
       HS2_PROF("ba_backsub", s);
@@ -1175,6 +1243,8 @@ extern "C" int hs2_ba_reduced_system(const float* poses, int64_t num_poses, cons
     return rc;
   const size_t n = 6 * (size_t)p.P;
   if (n > 0) {
+    ba_symmetrize_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>((int)n, w.A);
+    HS2_LAUNCH_CHECK("ba_symmetrize_kernel");
     HS2_CUDA(cudaMemcpyAsync(A_out, w.A, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
     HS2_CUDA(cudaMemcpyAsync(b_out, w.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   }

@@ -38,7 +38,8 @@ enum hs2_dtype { HS2_F32 = 0, HS2_F16 = 1, HS2_BF16 = 2, HS2_F64 = 3 };
 /* Bits of info[0] written on the device. */
 enum hs2_device_error {
   HS2_DEV_BAD_INDEX = 1, /* an edge index lies outside the pose/disparity buffers or >= t1 */
-  HS2_DEV_BAD_ETA = 2    /* eta has neither M nor 1 rows (M = #distinct depth frames) */
+  HS2_DEV_BAD_ETA = 2,   /* eta has neither M nor 1 rows (M = #distinct depth frames) */
+  HS2_DEV_TIMEOUT = 4    /* a bounded wait inside a kernel gave up (results are not valid) */
 };
 
 /* Message of the last failing call on this thread ("" if none). */

@@ -321,7 +321,7 @@ def ba(poses, disps, intrinsics, targets, weights, eta, ii, jj, t0, t1, iteratio
             C = accum_fast(lin["Cii"], ii, kx)
             w = accum_fast(lin["wi"], ii, kx)
             Q = 1.0 / (C + eta)
-            Ei = accum_fast(lin["Eii"].reshape(len(ii), -1), ii, ts).reshape(P, 6, HW)
+            Ei = accum_fast(lin["Eii"].reshape(len(ii), 6 * HW), ii, ts).reshape(P, 6, HW)
             E = np.concatenate([Ei, lin["Eij"]], axis=0)
             S, bS = schur_complement(E, Q, w, jj_exp, kk_exp, t0, t1)
             dx, ok = solve(A - S, b - bS, lm, ep)
