@@ -156,6 +156,8 @@ def accum_fast(data, ix, jx):
     data = np.asarray(data, dtype=np.float64)
     jx = np.asarray(jx, dtype=np.int64)
     ix = np.asarray(ix, dtype=np.int64)
+    if len(jx) == 0 or len(ix) == 0:
+        return np.zeros((len(jx),) + data.shape[1:], dtype=np.float64)
     order = np.argsort(jx)
     pos = np.searchsorted(jx[order], ix)
     pos = np.clip(pos, 0, len(jx) - 1)

@@ -270,3 +270,14 @@ def test_validation_rejects_out_of_window_indices():
         oba.validate(8, p["ii"], p["jj"], 2, 6)        # edges reach frame 7 >= t1
     with pytest.raises(ValueError):
         oba.validate(8, np.array([-1]), np.array([0]), 0, 8)
+
+
+def test_empty_window_and_no_edges():
+    p = small_problem()
+    r = oba.ba(p["poses"], p["disps"], p["intrinsics"], p["targets"], p["weights"], p["eta"], p["ii"], p["jj"],
+               8, 8, 1, p["lm"], p["ep"])
+    assert r.dx.shape == (0, 6) and r.dz.shape[0] == 8
+    e = np.zeros(0, dtype=np.int64)
+    r = oba.ba(p["poses"], p["disps"], p["intrinsics"], p["targets"][:0], p["weights"][:0], p["eta"][2:], e, e,
+               2, 8, 1, p["lm"], p["ep"])
+    assert np.all(r.dx == 0) and np.all(r.dz == 0)
