@@ -38,6 +38,8 @@ SIGNATURES = {
     "hs2_ba_workspace_size": [_i64, _i64, _i32, _i32, _i64, _i32, _i32, _i32, ctypes.POINTER(_sz)],
     "hs2_ba": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32, _i32,
                _f32, _f32, _i32, _p, _p, _i64, _p, _p, _sz, _p],
+    "hs2_ba_noalloc": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32, _i32,
+                       _f32, _f32, _i32, _p, _p, _i64, _p, _p],
     "hs2_ba_reduced_system": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32,
                               _i32, _p, _p, _p, _p, _sz, _p],
     "hs2_profile_enable": [_i32],

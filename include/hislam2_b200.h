@@ -129,6 +129,23 @@ int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num_disps, int
            int iterations, float lm, float ep, int motion_only, float* dx, float* dz, int64_t dz_rows,
            int32_t* info, void* workspace, size_t workspace_bytes, hs2_stream_t stream);
 
+/* ba without allocation.  No counterpart in the reference: this entry point is for
+ * callers that cannot allocate device memory when they run a BA step (a stream
+ * being captured into a CUDA graph, a process with a GPU memory budget fixed at
+ * start-up, a foreign-language host without a caching allocator).  Same arguments
+ * and results as hs2_ba, minus the workspace: the scratch is a static device array
+ * of 64 MiB inside the library, held by every GPU that loads it until exit.
+ * Problems whose hs2_ba_workspace_size() exceeds 64 MiB are rejected with
+ * HS2_ERR_WORKSPACE.  The first call on a device looks up the array's address
+ * (make that call before any stream capture).  All calls share the array, so calls
+ * whose GPU work overlaps in time race and must be serialised by the caller.
+ */
+int hs2_ba_noalloc(float* poses, int64_t num_poses, float* disps, int64_t num_disps, int ht, int wd,
+                   const float* intrinsics, const float* targets, const float* weights, const float* eta,
+                   int64_t eta_rows, const int64_t* ii, const int64_t* jj, int64_t num_edges, int t0,
+                   int t1, int iterations, float lm, float ep, int motion_only, float* dx, float* dz,
+                   int64_t dz_rows, int32_t* info, hs2_stream_t stream);
+
 /* Key generation of ba alone, for parity checks of the integer keys
  * (reference: src/droid_kernels.cu:1841-1849 unique/inverse, :1712-1740 schur rows).
  *   kx [min(num_poses,t1-t0+num_edges)] int32: sorted distinct frames of cat(arange(t0,t1), ii);
