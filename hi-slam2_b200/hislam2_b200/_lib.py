@@ -42,6 +42,7 @@ SIGNATURES = {
                        _f32, _f32, _i32, _p, _p, _i64, _p, _p],
     "hs2_ba_reduced_system": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32,
                               _i32, _p, _p, _p, _p, _sz, _p],
+    "hs2_ba_set_schur_path": [_i32],
     "hs2_profile_enable": [_i32],
     "hs2_launch_count": [],
     "hs2_profile_report": [ctypes.c_char_p, _sz, _i32],
@@ -103,3 +104,8 @@ def measure_simt_peaks():
 def launch_count():
     """Kernels launched by the library so far in this process."""
     return int(load().hs2_launch_count())
+
+
+def set_schur_path(path):
+    """0: tensor-core Schur Gram, 1: SIMT FP32 Schur Gram (default)."""
+    check(load().hs2_ba_set_schur_path(int(path)), "ba_set_schur_path")

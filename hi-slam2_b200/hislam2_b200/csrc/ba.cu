@@ -25,6 +25,7 @@
 // Only the (tiny) key generation is serial; everything else is sized by the
 // static problem dimensions, so a whole call is graph-capturable.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "common.cuh"
@@ -518,13 +519,13 @@ __device__ __forceinline__ void schur_scatter_block(double* A, int64_t n, int pa
 }
 
 __global__ void __launch_bounds__(256)
-ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, const int32_t* __restrict__ info) {
+ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int r0 = w.sptr[s];
   const int nr = w.sptr[s + 1] - r0;
-  if (nr == 0) return;
+  if (nr == 0 || nr < min_blocks) return;
   const int c0 = blockIdx.y * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
@@ -644,6 +645,261 @@ __global__ void ba_symmetrize_kernel(int n, double* __restrict__ A) {
   if (j > i) A[idx] = A[(int64_t)j * n + i];
 }
 
+// ------------------------------------------------------- schur (tcgen05) ---
+// Tensor-core form of the Schur Gram.  For depth frame k with Schur rows F (6
+// planes per row, HW pixels) the frame's block of the Gram is C = (Q o F_m) [F; w]^T,
+// a GEMM with K = pixels.  One CTA per (frame, 126-row M tile, pixel split):
+//   warps 0-3  stage 32 pixels of the rows per pipeline stage into shared memory
+//              in the canonical K-major 128B-swizzled layout, split into TF32
+//              hi/lo parts: A = Q*F rows of the M tile, B = all rows + the w row;
+//   warp 4     allocates 256 TMEM columns and (one elected lane) issues
+//              tcgen05.mma kind::tf32, M=128, N=Npad, K=8: A_hi.B_hi + A_hi.B_lo +
+//              A_lo.B_hi (3xTF32, ~FP32 products) into the TMEM accumulator;
+//              tcgen05.commit releases each stage and finally signals the epilogue;
+//   warps 0-3  read the accumulator (row per thread) and scatter the a <= b block
+//              pairs and the w column into the lower triangle of the FP64 system.
+// Frames with more than kTcMaxBlocks rows are left to the SIMT kernel.
+constexpr int kTcThreads = 160;
+constexpr int kTcK = 32;                       // pixels per stage (128 B per row)
+constexpr int kTcStages = 2;
+constexpr int kTcMBlocks = 21;                 // row blocks per M tile (126 rows)
+constexpr int kTcMaxBlocks = 42;               // N <= 6*42 + 1 <= 256
+constexpr int kTcNmax = 256;
+constexpr int kTcTileA = 128 * kTcK * 4;       // bytes of one A (hi or lo) tile
+constexpr int kTcTileB = kTcNmax * kTcK * 4;   // bytes of one B tile
+constexpr int kTcStageBytes = 2 * kTcTileA + 2 * kTcTileB;
+constexpr int kTcSmem = kTcStages * kTcStageBytes + 1024 /*align*/ + 2048 /*rows, bars*/;
+constexpr unsigned kTcSpin = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait; gives up (and raises *abort) after kTcSpin polls or when another
+// thread of the CTA already gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+  for (unsigned i = 0; i < kTcSpin; ++i) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  // K-major, 128B swizzle: LBO = 16 B (unused), SBO = 1024 B (8 rows x 128 B), version 1
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+__device__ __forceinline__ uint32_t umma_idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+// byte offset of (row r, pixel k) in a K-major 128B-swizzled tile
+__device__ __forceinline__ uint32_t sw128_off(int r, int k) {
+  return (uint32_t)(r * 128 + ((((k >> 2) ^ (r & 7)) & 7) << 4) + ((k & 3) << 2));
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const int r0 = w.sptr[s];
+  const int nr = w.sptr[s + 1] - r0;
+  const int mt = blockIdx.y;
+  if (nr == 0 || nr > kTcMaxBlocks || mt * kTcMBlocks >= nr) return;
+  const int c0 = blockIdx.z * chunk;
+  const int c1 = min(HW, c0 + chunk);
+  if (c0 >= c1) return;
+  const int na = min(kTcMBlocks, nr - mt * kTcMBlocks);  // row blocks of the A tile
+  const int nrowB = 6 * nr + 1;                             // + the w row
+  const int Npad = (nrowB + 15) & ~15;
+  const int nchunks = (c1 - c0 + kTcK - 1) / kTcK;
+
+  extern __shared__ uint8_t tc_raw[];
+  const uint32_t raw = smem_u32(tc_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* gbase = tc_raw + (base - raw);
+  uint8_t* meta = gbase + kTcStages * kTcStageBytes;
+  int* rowoffB = reinterpret_cast<int*>(meta);                 // [256] global plane offset / -1 / -2 (w)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(meta + 1024);    // full[2], empty[2], done
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 1024 + 64);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 1024 + 72);
+  const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + 2), bar_done = smem_u32(bars + 4);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int* srow = w.srow + r0;
+  const int* spose = w.spose + r0;
+  for (int r = tid; r < kTcNmax; r += kTcThreads) {
+    int v = -1;
+    if (r < 6 * nr) v = srow[r / 6] * 6 + (r % 6);
+    else if (r == 6 * nr) v = -2;
+    rowoffB[r] = v;
+  }
+  if (tid == 0) {
+    for (int q = 0; q < kTcStages; ++q) {
+      mbar_init(bar_full + 8 * q, 4);
+      mbar_init(bar_empty + 8 * q, 1);
+    }
+    mbar_init(bar_done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 4) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(256) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const float* Q = w.qbuf + (int64_t)s * HW;
+  const float* Wv = w.wbuf + (int64_t)s * HW;
+  const int arow0 = mt * 6 * kTcMBlocks;  // first B row of this M tile
+
+  if (warp < 4) {
+    // ------------------------------------------------------------- producers
+    for (int c = 0; c < nchunks; ++c) {
+      const int st = c % kTcStages;
+      const int use = c / kTcStages;
+      if (use > 0 && !mbar_wait(bar_empty + 8 * st, (use - 1) & 1, abort_flag)) break;
+      uint8_t* sA_hi = gbase + st * kTcStageBytes;
+      uint8_t* sA_lo = sA_hi + kTcTileA;
+      uint8_t* sB_hi = sA_lo + kTcTileA;
+      uint8_t* sB_lo = sB_hi + kTcTileB;
+      const int p = c0 + c * kTcK + lane;
+      const bool pin = p < c1;
+      const float q = pin ? Q[p] : 0.f;
+      for (int r = warp; r < Npad; r += 4) {
+        const int off = rowoffB[r];
+        float f = 0.f;
+        if (pin) {
+          if (off >= 0) f = w.erows[(int64_t)off * HW + p];
+          else if (off == -2) f = Wv[p];
+        }
+        const uint32_t o = sw128_off(r, lane);
+        const float fh = tf32_hi(f);
+        *reinterpret_cast<float*>(sB_hi + o) = fh;
+        *reinterpret_cast<float*>(sB_lo + o) = f - fh;
+        const int ra = r - arow0;
+        if (ra >= 0 && ra < 128) {
+          const float a = (ra < 6 * na && off >= 0) ? f * q : 0.f;
+          const float ah = tf32_hi(a);
+          const uint32_t oa = sw128_off(ra, lane);
+          *reinterpret_cast<float*>(sA_hi + oa) = ah;
+          *reinterpret_cast<float*>(sA_lo + oa) = a - ah;
+        }
+      }
+      // A rows of the tile that lie beyond the B rows (only when the tile is short)
+      for (int ra = warp; ra < 128; ra += 4) {
+        if (ra + arow0 < Npad) continue;
+        const uint32_t oa = sw128_off(ra, lane);
+        *reinterpret_cast<float*>(sA_hi + oa) = 0.f;
+        *reinterpret_cast<float*>(sA_lo + oa) = 0.f;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar_full + 8 * st);
+    }
+  } else if (lane == 0) {
+    // ------------------------------------------------------------- MMA issuer
+    const uint32_t idesc = umma_idesc_tf32(128, Npad);
+    for (int c = 0; c < nchunks; ++c) {
+      const int st = c % kTcStages;
+      if (!mbar_wait(bar_full + 8 * st, (c / kTcStages) & 1, abort_flag)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_hi = base + st * kTcStageBytes;
+      const uint32_t a_lo = a_hi + kTcTileA;
+      const uint32_t b_hi = a_lo + kTcTileA;
+      const uint32_t b_lo = b_hi + kTcTileB;
+#pragma unroll
+      for (int k = 0; k < kTcK / 8; ++k) {
+        const uint32_t kb = k * 32;
+        umma_tf32(tmem, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + kb), idesc, (c | k) ? 1u : 0u);
+        umma_tf32(tmem, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + kb), idesc, 1u);
+        umma_tf32(tmem, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + kb), idesc, 1u);
+      }
+      umma_commit(bar_empty + 8 * st);
+    }
+    umma_commit(bar_done);
+  }
+
+  // ------------------------------------------------------------- epilogue
+  bool ok = true;
+  if (warp < 4) {
+    ok = mbar_wait(bar_done, 0, abort_flag);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int m = warp * 32 + lane;                 // accumulator row = TMEM lane
+    const int64_t n = 6 * (int64_t)P;
+    const bool mrow = ok && m < 6 * na;
+    const int a = mt * kTcMBlocks + m / 6, x = m % 6;
+    const int pa = mrow ? spose[a] : 0;
+    for (int col0 = 0; col0 < Npad; col0 += 16) {
+      uint32_t v[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!mrow) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int col = col0 + j;
+        const double val = -(double)__uint_as_float(v[j]);
+        if (col < 6 * nr) {
+          const int b = col / 6, y = col % 6;
+          if (b < a) continue;
+          const int pb = spose[b];
+          if (pa > pb) atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], val);
+          else if (pa < pb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], val);
+          else {
+            atomicAdd(&w.A[(pa * 6 + x) * n + pa * 6 + y], val);
+            if (a != b) atomicAdd(&w.A[(pa * 6 + y) * n + pa * 6 + x], val);
+          }
+        } else if (col == 6 * nr) {
+          atomicAdd(&w.b[pa * 6 + x], val);
+        }
+      }
+    }
+  }
+  if (*abort_flag && tid == 0) atomicOr(info, HS2_DEV_TIMEOUT);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 4) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
 // ------------------------------------------------------------- cholesky ---
 // Damped FP64 Cholesky factorisation + solve of the reduced camera system in one
 // cooperative (persistent) launch.  Phases are separated by a grid barrier:
@@ -672,6 +928,10 @@ struct CholBuf {
   double* y;        // [n] forward-substituted right-hand side
   unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed
 };
+
+__device__ __forceinline__ double2 ldcg2(const double* p) {
+  return __ldcg(reinterpret_cast<const double2*>(p));
+}
 
 __device__ __forceinline__ bool grid_barrier(unsigned* ctl, unsigned nblocks, int32_t* info) {
   __shared__ int s_ok;
@@ -845,10 +1105,23 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
       const int ri = o + kNB + I * kNB, rj = o + kNB + J * kNB;
       const int ni = min(kNB, n - ri), nj = min(kNB, n - rj);
       __syncthreads();
-      for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
-        const int a = idx >> 6, k = idx & 63;
-        Ai[a][k] = a < ni ? __ldcg(&A[(int64_t)(ri + a) * n + o + k]) : 0.0;
-        Aj[a][k] = a < nj ? __ldcg(&A[(int64_t)(rj + a) * n + o + k]) : 0.0;
+      {
+        // 2 x 64x64 doubles, 16 independent loads in flight per thread
+        double2 va[8], vb[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int idx = tid + q * kCholThreads;  // double2 index in the 64x32 grid
+          const int a = idx >> 5, k = (idx & 31) * 2;
+          va[q] = a < ni ? ldcg2(&A[(int64_t)(ri + a) * n + o + k]) : make_double2(0.0, 0.0);
+          vb[q] = a < nj ? ldcg2(&A[(int64_t)(rj + a) * n + o + k]) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int idx = tid + q * kCholThreads;
+          const int a = idx >> 5, k = (idx & 31) * 2;
+          Ai[a][k] = va[q].x; Ai[a][k + 1] = va[q].y;
+          Aj[a][k] = vb[q].x; Aj[a][k + 1] = vb[q].y;
+        }
       }
       __syncthreads();
       double acc[4][4];
@@ -886,19 +1159,35 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
   if (!failed) {
     double (*Ls)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm);
     double* ys = csm + kNB * (kNB + 1);
+    double* dv = ys + kNB;
+    double* part = dv + kNB;  // [4][64] partial sums of the update
     for (int kb = nbk - 1; kb >= 0; --kb) {
       const int o = kb * kNB;
       const int nb = min(kNB, n - o);
       __syncthreads();
-      for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
-        const int i = idx >> 6, l = idx & 63;
-        Ls[i][l] = __ldcg(&cb.L11[((int64_t)kb * kNB + i) * kNB + l]);
+      {
+        double2 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int idx = tid + q * kCholThreads;
+          v[q] = ldcg2(&cb.L11[((int64_t)kb * kNB + (idx >> 5)) * kNB + (idx & 31) * 2]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int idx = tid + q * kCholThreads;
+          Ls[idx >> 5][(idx & 31) * 2] = v[q].x;
+          Ls[idx >> 5][(idx & 31) * 2 + 1] = v[q].y;
+        }
       }
-      for (int i = tid; i < nb; i += kCholThreads) ys[i] = __ldcg(&cb.y[o + i]);
+      if (tid < kNB) {
+        ys[tid] = tid < nb ? __ldcg(&cb.y[o + tid]) : 0.0;
+        dv[tid] = tid < nb ? __ldcg(&cb.dinv[(int64_t)kb * kNB + tid]) : 0.0;
+      }
       __syncthreads();
       if (tid < 32) {
+        // x = L11^-T y, column-oriented on L11^T (row j of L11)
         for (int j = nb - 1; j >= 0; --j) {
-          const double xj = ys[j] * __ldcg(&cb.dinv[(int64_t)kb * kNB + j]);
+          const double xj = ys[j] * dv[j];
           __syncwarp();
           if (tid == 0) ys[j] = xj;
           for (int i = tid; i < j; i += 32) ys[i] -= Ls[j][i] * xj;
@@ -908,10 +1197,28 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
       __syncthreads();
       if (blockIdx.x == 0)
         for (int i = tid; i < nb; i += kCholThreads) w.x[o + i] = ys[i];
-      for (int c = blockIdx.x * kCholThreads + tid; c < o; c += G * kCholThreads) {
-        double s = 0.0;
-        for (int r = 0; r < nb; ++r) s += __ldcg(&A[(int64_t)(o + r) * n + c]) * ys[r];
-        cb.y[c] = __ldcg(&cb.y[c]) - s;
+      // y_c -= sum_r L[o+r][c] x_r for c < o: 64 columns per CTA, 4 x 16 rows per column
+      const int cl = tid & 63, rg = tid >> 6;
+      for (int c0 = blockIdx.x * kNB; c0 < o; c0 += G * kNB) {
+        const int c = c0 + cl;
+        double sacc = 0.0;
+        if (c < o) {
+          double lv[16];
+#pragma unroll
+          for (int r = 0; r < 16; ++r) {
+            const int row = rg * 16 + r;
+            lv[r] = row < nb ? __ldcg(&A[(int64_t)(o + row) * n + c]) : 0.0;
+          }
+#pragma unroll
+          for (int r = 0; r < 16; ++r) sacc += lv[r] * ys[rg * 16 + r];
+        }
+        part[rg * kNB + cl] = sacc;
+        __syncthreads();
+        if (rg == 0 && c < o) {
+          const double tot = part[cl] + part[kNB + cl] + part[2 * kNB + cl] + part[3 * kNB + cl];
+          cb.y[c] = __ldcg(&cb.y[c]) - tot;
+        }
+        __syncthreads();
       }
       if (!grid_barrier(cb.ctl, G, info)) return;
     }
@@ -1062,8 +1369,12 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
 }
 
 struct BaLaunch {
-  int nchunk, schur_split, schur_chunk;
+  int nchunk, schur_split, schur_chunk, tc_split, tc_chunk;
 };
+
+// Schur Gram path: 0 = tensor cores (3xTF32) with the SIMT kernel for frames of more
+// than kTcMaxBlocks rows; 1 = SIMT FP32 for every frame.
+static std::atomic<int> g_schur_path{1};
 
 static BaLaunch ba_launch_shape(const BaProblem& p) {
   BaLaunch l;
@@ -1075,6 +1386,12 @@ static BaLaunch ba_launch_shape(const BaProblem& p) {
   l.schur_chunk = (p.HW + l.schur_split - 1) / l.schur_split;
   l.schur_chunk = (l.schur_chunk + kSchurTP - 1) / kSchurTP * kSchurTP;
   l.schur_split = (p.HW + l.schur_chunk - 1) / l.schur_chunk;
+  // tensor-core split: about 4 waves of one-CTA-per-SM work units, >= 64 pixels each
+  l.tc_split = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, p.HW / 64),
+                                                           (4 * kNumSMs + S - 1) / std::max<int64_t>(S, 1)));
+  l.tc_chunk = (p.HW + l.tc_split - 1) / l.tc_split;
+  l.tc_chunk = (l.tc_chunk + kTcK - 1) / kTcK * kTcK;
+  l.tc_split = (p.HW + l.tc_chunk - 1) / l.tc_chunk;
   return l;
 }
 
@@ -1112,9 +1429,22 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
     HS2_LAUNCH_CHECK("ba_assemble_kernel");
   }
   if (!p.motion_only && n > 0 && S > 0) {
-    dim3 grid((unsigned)S, l.schur_split);
     HS2_PROF("ba_schur", s);
-    ba_schur_kernel<<<grid, 256, 0, s>>>(p.HW, l.schur_chunk, w, P, info);
+    const bool simt_only = g_schur_path.load() == 1;
+    if (!simt_only) {
+      static bool attr_set[64] = {false};
+      int dev = 0;
+      HS2_CUDA(cudaGetDevice(&dev));
+      if (dev < 64 && !attr_set[dev]) {
+        HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        attr_set[dev] = true;
+      }
+      dim3 grid((unsigned)S, (unsigned)((kTcMaxBlocks + kTcMBlocks - 1) / kTcMBlocks), l.tc_split);
+      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(p.HW, l.tc_chunk, w, P, info);
+      HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
+    }
+    dim3 grid((unsigned)S, l.schur_split);
+    ba_schur_kernel<<<grid, 256, 0, s>>>(p.HW, l.schur_chunk, w, P, simt_only ? 1 : kTcMaxBlocks + 1, info);
     HS2_LAUNCH_CHECK("ba_schur_kernel");
   }
   return HS2_OK;
@@ -1248,5 +1578,15 @@ extern "C" int hs2_ba_reduced_system(const float* poses, int64_t num_poses, cons
     HS2_CUDA(cudaMemcpyAsync(A_out, w.A, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
     HS2_CUDA(cudaMemcpyAsync(b_out, w.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   }
+  return HS2_OK;
+}
+
+extern "C" int hs2_ba_set_schur_path(int path) {
+  using namespace hs2;
+  if (path != 0 && path != 1) {
+    set_error("ba_set_schur_path: path must be 0 (tensor cores) or 1 (SIMT FP32)");
+    return HS2_ERR_INVALID;
+  }
+  g_schur_path.store(path);
   return HS2_OK;
 }

@@ -173,6 +173,15 @@ int hs2_ba_reduced_system(const float* poses, int64_t num_poses, const float* di
                           double* A_out, double* b_out, int32_t* info, void* workspace,
                           size_t workspace_bytes, hs2_stream_t stream);
 
+/* Selects the kernel of the Schur Gram for later hs2_ba calls (process-wide; no
+ * counterpart in the reference, whose Gram is SIMT FP32 in EEt6x6_kernel):
+ *   0 tensor cores, tcgen05 kind::tf32 with a hi/lo split of both operands
+ *     (3 products, about FP32 accuracy) -- depth frames with more than 42 Schur rows
+ *     fall back to the SIMT kernel;
+ *   1 (default) SIMT FP32 for every frame.
+ */
+int hs2_ba_set_schur_path(int path);
+
 /* ---------------------------------------------------------------------------
  * Measurement support (no counterpart in the reference, which has no profiler).
  * hs2_profile_enable(1) brackets every kernel launch of this library with CUDA

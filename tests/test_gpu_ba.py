@@ -70,16 +70,41 @@ def oracle_reduced_system(p, motion_only=False):
     return it["A"] - it["S"], it["b"] - it["bS"]
 
 
+def star_problem():
+    """60 frames of the 300-kf workload plus 48 edges out of frame 12: its depth frame has
+    49 Schur rows, past the tensor-core Gram's limit of 42, so both Gram kernels run."""
+    p = subproblem(synth.make_ba_problem("backend300", seed=3), 60)
+    extra_j = torch.arange(13, 61) % 60
+    extra_j[extra_j == 12] = 0
+    extra_i = torch.full_like(extra_j, 12)
+    coords = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], extra_i, extra_j)
+    q = dict(p)
+    q["ii"] = torch.cat([p["ii"], extra_i])
+    q["jj"] = torch.cat([p["jj"], extra_j])
+    q["targets"] = torch.cat([p["targets"], coords.permute(0, 3, 1, 2).float()]).contiguous()
+    q["weights"] = torch.cat([p["weights"], torch.full_like(p["weights"][:48], 0.5)]).contiguous()
+    return q
+
+
 CASES = {
     "frontend_small": lambda: synth.make_ba_problem("frontend_small", seed=0),
     "frontend": lambda: synth.make_ba_problem("frontend", seed=1),
     "backend40": lambda: subproblem(synth.make_ba_problem("backend300", seed=2), 40),
+    "star60": star_problem,
 }
+
+
+@pytest.fixture(params=[0, 1], ids=["gram_tc", "gram_simt"])
+def schur_path(request):
+    from hislam2_b200 import _lib
+    _lib.set_schur_path(request.param)
+    yield request.param
+    _lib.set_schur_path(1)
 
 
 @pytest.mark.parametrize("case", list(CASES))
 @pytest.mark.parametrize("motion_only", [False, True])
-def test_reduced_system_matches_oracle(cuda, case, motion_only):
+def test_reduced_system_matches_oracle(cuda, case, motion_only, schur_path):
     p = CASES[case]()
     q = on(p, cuda)
     A, b = backends.ba_reduced_system(q["poses"], q["disps"], q["intrinsics"], q["targets"], q["weights"],
@@ -92,7 +117,7 @@ def test_reduced_system_matches_oracle(cuda, case, motion_only):
 
 
 @pytest.mark.parametrize("case", list(CASES))
-def test_ba_matches_oracle(cuda, case):
+def test_ba_matches_oracle(cuda, case, schur_path):
     p = CASES[case]()
     poses, disps, dx, dz = run_gpu(p, cuda)
     r = run_oracle(p)
