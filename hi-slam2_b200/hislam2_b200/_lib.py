@@ -107,5 +107,5 @@ def launch_count():
 
 
 def set_schur_path(path):
-    """0: tensor-core Schur Gram, 1: SIMT FP32 Schur Gram (default)."""
+    """0: tensor-core Schur Gram (default), 1: SIMT FP32 Schur Gram."""
     check(load().hs2_ba_set_schur_path(int(path)), "ba_set_schur_path")

@@ -28,6 +28,8 @@
 #include <atomic>
 #include <cstring>
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "profile.cuh"
 
@@ -42,11 +44,15 @@ constexpr int kEtab = 48;                           // floats per edge in the ed
 
 // ------------------------------------------------------------ workspace ---
 struct BaLayout {
-  size_t flag, slot, kx, gptr, gedge, cursor, rptr, rrow, rpose, sptr, srow, spose;
+  size_t flag, slot, kx, gptr, gedge, cursor, rptr, rrow, rpose, sptr, srow, spose, epos, wpos;
   size_t etab, etab64, hedge, erows, qbuf, wbuf, A, b, x, chol_fail, L11, dinv, ychol, ctl, total;
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Row stride (floats) of the E-row planes: pixels padded to 32 so that every plane
+// row starts on a 128-byte boundary (TMA tiles of 32 pixels).
+static __host__ __device__ __forceinline__ int row_stride(int HW) { return (HW + 31) & ~31; }
 
 static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) {
   BaLayout L;
@@ -67,10 +73,12 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
   L.sptr = take(sizeof(int) * (S + 2));
   L.srow = take(sizeof(int) * (R + 1));
   L.spose = take(sizeof(int) * (R + 1));
+  L.epos = take(sizeof(int) * (E + 1));
+  L.wpos = take(sizeof(int) * (P + 1));
   L.etab = take(sizeof(float) * kEtab * (E + 1));
   L.etab64 = take(sizeof(double) * 36 * (E + 1));
   L.hedge = take(sizeof(double) * 27 * (E + 1));
-  L.erows = take(motion_only ? 0 : sizeof(float) * 6 * (size_t)R * HW);
+  L.erows = take(motion_only ? 0 : sizeof(float) * 6 * (size_t)R * row_stride(HW));
   L.qbuf = take(motion_only ? 0 : sizeof(float) * (size_t)S * HW);
   L.wbuf = take(motion_only ? 0 : sizeof(float) * (size_t)S * HW);
   L.A = take(sizeof(double) * (size_t)(n * n + 1));
@@ -86,7 +94,7 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
 }
 
 struct BaPtrs {
-  int *flag, *slot, *kx, *gptr, *gedge, *cursor, *rptr, *rrow, *rpose, *sptr, *srow, *spose;
+  int *flag, *slot, *kx, *gptr, *gedge, *cursor, *rptr, *rrow, *rpose, *sptr, *srow, *spose, *epos, *wpos;
   float* etab;
   double *etab64, *hedge;
   float *erows, *qbuf, *wbuf;
@@ -109,6 +117,8 @@ static BaPtrs ba_ptrs(void* ws, const BaLayout& L) {
   p.sptr = (int*)(base + L.sptr);
   p.srow = (int*)(base + L.srow);
   p.spose = (int*)(base + L.spose);
+  p.epos = (int*)(base + L.epos);
+  p.wpos = (int*)(base + L.wpos);
   p.etab = (float*)(base + L.etab);
   p.etab64 = (double*)(base + L.etab64);
   p.hedge = (double*)(base + L.hedge);
@@ -238,18 +248,27 @@ ba_keys_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, i
   __syncthreads();
   block_exclusive_scan(w.rptr, M + 1, sh);
   block_exclusive_scan(w.sptr, M + 1, sh);
+  // E rows are stored depth-frame-major in this list order: a frame's Schur rows
+  // first (same order as its srow list), then its rows whose pose is not optimised.
   for (int s = threadIdx.x; s < M; s += 1024) {
     const int f = w.kx[s];
     int r = w.rptr[s], q = w.sptr[s];
     if (f >= t0 && f < t1) {
-      w.rrow[r] = f - t0; w.rpose[r] = f - t0; ++r;
+      w.rrow[r] = f - t0; w.rpose[r] = f - t0; w.wpos[f - t0] = r; ++r;
       w.srow[q] = f - t0; w.spose[q] = f - t0; ++q;
     }
     for (int g = w.gptr[s]; g < w.gptr[s + 1]; ++g) {
       const int e = w.gedge[g];
       const int pj = (int)(jj[e] - t0);
-      w.rrow[r] = P + e; w.rpose[r] = pj; ++r;
-      if (pj >= 0 && pj < P) { w.srow[q] = P + e; w.spose[q] = pj; ++q; }
+      if (pj >= 0 && pj < P) {
+        w.rrow[r] = P + e; w.rpose[r] = pj; w.epos[e] = r; ++r;
+        w.srow[q] = P + e; w.spose[q] = pj; ++q;
+      }
+    }
+    for (int g = w.gptr[s]; g < w.gptr[s + 1]; ++g) {
+      const int e = w.gedge[g];
+      const int pj = (int)(jj[e] - t0);
+      if (!(pj >= 0 && pj < P)) { w.rrow[r] = P + e; w.rpose[r] = pj; w.epos[e] = r; ++r; }
     }
   }
 }
@@ -304,6 +323,7 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
   const int M = info[1];
   if (s >= M) return;
   const int P = t1 - t0;
+  const int HWs = row_stride(HW);
   const int f = w.kx[s];
   const bool inwin = f >= t0 && f < t1;
   const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
@@ -334,7 +354,7 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
     const float q[4] = {tab[3], tab[4], tab[5], tab[6]};
     const float* trg = targets + (int64_t)e * 2 * HW;
     const float* wgt = weights + (int64_t)e * 2 * HW;
-    float* Erow = w.erows + ((int64_t)(P + e) * 6) * HW;
+    float* Erow = w.erows + ((int64_t)w.epos[e] * 6) * HWs;
 
     float H[27];
 #pragma unroll
@@ -385,7 +405,7 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
 #pragma unroll
         for (int r = 0; r < 6; ++r) {
           Ej[r] = zu * Ju[r] + zv * Jv[r];
-          Erow[(int64_t)r * HW + p] = Ej[r];
+          Erow[(int64_t)r * HWs + p] = Ej[r];
         }
         if (inwin) {
 #pragma unroll
@@ -423,9 +443,9 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
     w.qbuf[(int64_t)s * HW + p] = 1.0f / (Cs[k] + eta_row[p]);
     w.wbuf[(int64_t)s * HW + p] = Ws[k];
     if (inwin) {
-      float* Er = w.erows + ((int64_t)(f - t0) * 6) * HW;
+      float* Er = w.erows + ((int64_t)w.wpos[f - t0] * 6) * HWs;
 #pragma unroll
-      for (int r = 0; r < 6; ++r) Er[(int64_t)r * HW + p] = Ei[k][r];
+      for (int r = 0; r < 6; ++r) Er[(int64_t)r * HWs + p] = Ei[k][r];
     }
   }
 }
@@ -529,8 +549,9 @@ ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, const int32_
   const int c0 = blockIdx.y * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
-  const int* srow = w.srow + r0;
   const int* spose = w.spose + r0;
+  const int rbase = w.rptr[s];          // storage position of the frame's first Schur row
+  const int HWs = row_stride(HW);
   const int64_t n = 6 * (int64_t)P;
   const float* Q = w.qbuf + (int64_t)s * HW;
   const float* W = w.wbuf + (int64_t)s * HW;
@@ -585,8 +606,8 @@ ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, const int32_
           const int blk = row / 6, d = row - (row / 6) * 6;
           float va = 0.f, vb = 0.f;
           if (p < c1) {
-            if (blk < na) va = w.erows[((int64_t)srow[mt * kSchurTB + blk] * 6 + d) * HW + p] * Q[p];
-            if (blk < nb) vb = w.erows[((int64_t)srow[nt * kSchurTB + blk] * 6 + d) * HW + p];
+            if (blk < na) va = w.erows[((int64_t)(rbase + mt * kSchurTB + blk) * 6 + d) * HWs + p] * Q[p];
+            if (blk < nb) vb = w.erows[((int64_t)(rbase + nt * kSchurTB + blk) * 6 + d) * HWs + p];
           }
           Fa[pp][row] = va;
           Fb[pp][row] = vb;
@@ -646,29 +667,34 @@ __global__ void ba_symmetrize_kernel(int n, double* __restrict__ A) {
 }
 
 // ------------------------------------------------------- schur (tcgen05) ---
-// Tensor-core form of the Schur Gram.  For depth frame k with Schur rows F (6
-// planes per row, HW pixels) the frame's block of the Gram is C = (Q o F_m) [F; w]^T,
-// a GEMM with K = pixels.  One CTA per (frame, 126-row M tile, pixel split):
-//   warps 0-3  stage 32 pixels of the rows per pipeline stage into shared memory
-//              in the canonical K-major 128B-swizzled layout, split into TF32
-//              hi/lo parts: A = Q*F rows of the M tile, B = all rows + the w row;
-//   warp 4     allocates 256 TMEM columns and (one elected lane) issues
-//              tcgen05.mma kind::tf32, M=128, N=Npad, K=8: A_hi.B_hi + A_hi.B_lo +
-//              A_lo.B_hi (3xTF32, ~FP32 products) into the TMEM accumulator;
-//              tcgen05.commit releases each stage and finally signals the epilogue;
-//   warps 0-3  read the accumulator (row per thread) and scatter the a <= b block
-//              pairs and the w column into the lower triangle of the FP64 system.
-// Frames with more than kTcMaxBlocks rows are left to the SIMT kernel.
-constexpr int kTcThreads = 160;
-constexpr int kTcK = 32;                       // pixels per stage (128 B per row)
-constexpr int kTcStages = 2;
-constexpr int kTcMBlocks = 21;                 // row blocks per M tile (126 rows)
+// Tensor-core form of the Schur Gram.  With G = sqrt(Q) o F (the frame's Schur rows
+// scaled per pixel) the frame's block of the Gram is S = G G^T and its rhs column is
+// v = G (sqrt(Q) w): one symmetric GEMM per depth frame with K = pixels, B = [G; sqrt(Q) w]
+// and A = a 128-row window of the same shared-memory tile.  One CTA per (frame, 128-row
+// M tile, pixel split):
+//   warp 9     TMA: per 32-pixel chunk, up to four 64x32 fp32 boxes of the frame's E
+//              planes (stored contiguously, depth-frame-major) land 128B-swizzled in
+//              the stage's hi tile (cp.async.bulk.tensor, mbarrier complete_tx);
+//   warps 0-7  scale by sqrt(Q), add the w row, zero the padding and split each value
+//              into TF32 hi/lo parts in place (8 rows in flight per thread);
+//   warp 8     allocates 256 TMEM columns; one lane issues tcgen05.mma kind::tf32
+//              M=128, N=Npad, K=8: A_hi.B_hi + A_hi.B_lo + A_lo.B_hi (3xTF32) and
+//              tcgen05.commit releases the stage / finally signals the epilogue;
+//   warps 0-7  read the accumulator (warp w: TMEM lanes of quarter w%4, column half w/4)
+//              and scatter the a <= b block pairs and the v column into the lower
+//              triangle of the FP64 system.
+// Three stages of 64 KB; every mbarrier wait is bounded (HS2_DEV_TIMEOUT).  Frames with
+// more than kTcMaxBlocks Schur rows are left to the SIMT kernel.  Requires Q >= 0 (eta > 0).
+constexpr int kTcThreads = 320;
+constexpr int kTcSplitWarps = 8;
+constexpr int kTcK = 32;                       // pixels per stage (128 B per plane row)
+constexpr int kTcStages = 3;
 constexpr int kTcMaxBlocks = 42;               // N <= 6*42 + 1 <= 256
-constexpr int kTcNmax = 256;
-constexpr int kTcTileA = 128 * kTcK * 4;       // bytes of one A (hi or lo) tile
-constexpr int kTcTileB = kTcNmax * kTcK * 4;   // bytes of one B tile
-constexpr int kTcStageBytes = 2 * kTcTileA + 2 * kTcTileB;
-constexpr int kTcSmem = kTcStages * kTcStageBytes + 1024 /*align*/ + 2048 /*rows, bars*/;
+constexpr int kTcRows = 256;                   // plane rows per tile
+constexpr int kTcBox = 64;                     // plane rows per TMA box
+constexpr int kTcTile = kTcRows * kTcK * 4;    // 32 KB
+constexpr int kTcStageBytes = 2 * kTcTile;     // hi + lo
+constexpr int kTcSmem = kTcStages * kTcStageBytes + 1024 /*align*/ + 2048 /*barriers*/;
 constexpr unsigned kTcSpin = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -679,6 +705,10 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
 }
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+               "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
   uint32_t ok;
@@ -696,6 +726,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
   }
   *abort = 1;
   return false;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
 }
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   // K-major, 128B swizzle: LBO = 16 B (unused), SBO = 1024 B (8 rows x 128 B), version 1
@@ -720,58 +755,53 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
-// byte offset of (row r, pixel k) in a K-major 128B-swizzled tile
+// byte offset of (row r, pixel k) in a K-major 128B-swizzled tile (1024-byte aligned)
 __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
   return (uint32_t)(r * 128 + ((((k >> 2) ^ (r & 7)) & 7) << 4) + ((k & 3) << 2));
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ info) {
+ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, BaPtrs w, int P,
+                   int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
-  const int r0 = w.sptr[s];
-  const int nr = w.sptr[s + 1] - r0;
+  const int nr = w.sptr[s + 1] - w.sptr[s];
   const int mt = blockIdx.y;
-  if (nr == 0 || nr > kTcMaxBlocks || mt * kTcMBlocks >= nr) return;
+  if (nr == 0 || nr > kTcMaxBlocks || mt * 128 >= 6 * nr) return;
   const int c0 = blockIdx.z * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
-  const int na = min(kTcMBlocks, nr - mt * kTcMBlocks);  // row blocks of the A tile
-  const int nrowB = 6 * nr + 1;                             // + the w row
+  const int nrowB = 6 * nr + 1;                   // + the sqrt(Q) w row
   const int Npad = (nrowB + 15) & ~15;
+  const int nbox = (6 * nr + kTcBox - 1) / kTcBox;
   const int nchunks = (c1 - c0 + kTcK - 1) / kTcK;
+  const int prow0 = w.rptr[s] * 6;                 // first plane row of the frame's Schur rows
 
   extern __shared__ uint8_t tc_raw[];
   const uint32_t raw = smem_u32(tc_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* gbase = tc_raw + (base - raw);
   uint8_t* meta = gbase + kTcStages * kTcStageBytes;
-  int* rowoffB = reinterpret_cast<int*>(meta);                 // [256] global plane offset / -1 / -2 (w)
-  uint64_t* bars = reinterpret_cast<uint64_t*>(meta + 1024);    // full[2], empty[2], done
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 1024 + 64);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 1024 + 72);
-  const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + 2), bar_done = smem_u32(bars + 4);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(meta);  // tma[3], full[3], empty[3], done
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 128);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 136);
+  const uint32_t bar_tma = smem_u32(bars), bar_full = smem_u32(bars + 3), bar_empty = smem_u32(bars + 6);
+  const uint32_t bar_done = smem_u32(bars + 9);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int* srow = w.srow + r0;
-  const int* spose = w.spose + r0;
-  for (int r = tid; r < kTcNmax; r += kTcThreads) {
-    int v = -1;
-    if (r < 6 * nr) v = srow[r / 6] * 6 + (r % 6);
-    else if (r == 6 * nr) v = -2;
-    rowoffB[r] = v;
-  }
+  const int* spose = w.spose + w.sptr[s];
   if (tid == 0) {
     for (int q = 0; q < kTcStages; ++q) {
-      mbar_init(bar_full + 8 * q, 4);
+      mbar_init(bar_tma + 8 * q, 1);
+      mbar_init(bar_full + 8 * q, kTcSplitWarps);
       mbar_init(bar_empty + 8 * q, 1);
     }
     mbar_init(bar_done, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 4) {
+  if (warp == kTcSplitWarps) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(256) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -782,47 +812,56 @@ ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ inf
   const uint32_t tmem = *tmem_slot;
   const float* Q = w.qbuf + (int64_t)s * HW;
   const float* Wv = w.wbuf + (int64_t)s * HW;
-  const int arow0 = mt * 6 * kTcMBlocks;  // first B row of this M tile
 
-  if (warp < 4) {
-    // ------------------------------------------------------------- producers
+  if (warp == kTcSplitWarps + 1) {
+    // ------------------------------------------------------------- TMA producer
+    if (lane == 0) {
+      const uint32_t bytes = (uint32_t)nbox * kTcBox * kTcK * 4;
+      for (int c = 0; c < nchunks; ++c) {
+        const int st = c % kTcStages;
+        const int use = c / kTcStages;
+        if (use > 0 && !mbar_wait(bar_empty + 8 * st, (use - 1) & 1, abort_flag)) break;
+        mbar_arrive_tx(bar_tma + 8 * st, bytes);
+        const uint32_t dst = base + st * kTcStageBytes;
+        for (int i = 0; i < nbox; ++i)
+          tma_load_2d(dst + i * kTcBox * 128, &emap, c0 + c * kTcK, prow0 + i * kTcBox, bar_tma + 8 * st);
+      }
+    }
+  } else if (warp < kTcSplitWarps) {
+    // ------------------------------------------------------------- split
+    int pn = c0 + lane;
+    float qn = pn < c1 ? Q[pn] : 0.f, wn = pn < c1 ? Wv[pn] : 0.f;
     for (int c = 0; c < nchunks; ++c) {
       const int st = c % kTcStages;
-      const int use = c / kTcStages;
-      if (use > 0 && !mbar_wait(bar_empty + 8 * st, (use - 1) & 1, abort_flag)) break;
-      uint8_t* sA_hi = gbase + st * kTcStageBytes;
-      uint8_t* sA_lo = sA_hi + kTcTileA;
-      uint8_t* sB_hi = sA_lo + kTcTileA;
-      uint8_t* sB_lo = sB_hi + kTcTileB;
-      const int p = c0 + c * kTcK + lane;
-      const bool pin = p < c1;
-      const float q = pin ? Q[p] : 0.f;
-      for (int r = warp; r < Npad; r += 4) {
-        const int off = rowoffB[r];
-        float f = 0.f;
-        if (pin) {
-          if (off >= 0) f = w.erows[(int64_t)off * HW + p];
-          else if (off == -2) f = Wv[p];
+      const float sq = sqrtf(fmaxf(qn, 0.f));
+      const float wq = wn * sq;
+      // prefetch Q, w of the next chunk
+      pn = c0 + (c + 1) * kTcK + lane;
+      qn = pn < c1 ? Q[pn] : 0.f;
+      wn = pn < c1 ? Wv[pn] : 0.f;
+      if (!mbar_wait(bar_tma + 8 * st, (c / kTcStages) & 1, abort_flag)) break;
+      uint8_t* hi = gbase + st * kTcStageBytes;
+      uint8_t* lo = hi + kTcTile;
+      for (int rb = warp; rb < Npad; rb += 8 * kTcSplitWarps) {
+        float g[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = rb + u * kTcSplitWarps;
+          float v = 0.f;
+          if (r < 6 * nr) v = *reinterpret_cast<const float*>(hi + sw128_off(r, lane)) * sq;
+          else if (r == 6 * nr) v = wq;
+          g[u] = v;
         }
-        const uint32_t o = sw128_off(r, lane);
-        const float fh = tf32_hi(f);
-        *reinterpret_cast<float*>(sB_hi + o) = fh;
-        *reinterpret_cast<float*>(sB_lo + o) = f - fh;
-        const int ra = r - arow0;
-        if (ra >= 0 && ra < 128) {
-          const float a = (ra < 6 * na && off >= 0) ? f * q : 0.f;
-          const float ah = tf32_hi(a);
-          const uint32_t oa = sw128_off(ra, lane);
-          *reinterpret_cast<float*>(sA_hi + oa) = ah;
-          *reinterpret_cast<float*>(sA_lo + oa) = a - ah;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int r = rb + u * kTcSplitWarps;
+          if (r < Npad) {
+            const uint32_t o = sw128_off(r, lane);
+            const float gh = tf32_hi(g[u]);
+            *reinterpret_cast<float*>(hi + o) = gh;
+            *reinterpret_cast<float*>(lo + o) = g[u] - gh;
+          }
         }
-      }
-      // A rows of the tile that lie beyond the B rows (only when the tile is short)
-      for (int ra = warp; ra < 128; ra += 4) {
-        if (ra + arow0 < Npad) continue;
-        const uint32_t oa = sw128_off(ra, lane);
-        *reinterpret_cast<float*>(sA_hi + oa) = 0.f;
-        *reinterpret_cast<float*>(sA_lo + oa) = 0.f;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -835,10 +874,10 @@ ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ inf
       const int st = c % kTcStages;
       if (!mbar_wait(bar_full + 8 * st, (c / kTcStages) & 1, abort_flag)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a_hi = base + st * kTcStageBytes;
-      const uint32_t a_lo = a_hi + kTcTileA;
-      const uint32_t b_hi = a_lo + kTcTileA;
-      const uint32_t b_lo = b_hi + kTcTileB;
+      const uint32_t b_hi = base + st * kTcStageBytes;
+      const uint32_t b_lo = b_hi + kTcTile;
+      const uint32_t a_hi = b_hi + mt * 128 * 128;
+      const uint32_t a_lo = b_lo + mt * 128 * 128;
 #pragma unroll
       for (int k = 0; k < kTcK / 8; ++k) {
         const uint32_t kb = k * 32;
@@ -852,18 +891,18 @@ ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ inf
   }
 
   // ------------------------------------------------------------- epilogue
-  bool ok = true;
-  if (warp < 4) {
-    ok = mbar_wait(bar_done, 0, abort_flag);
+  if (warp < kTcSplitWarps) {
+    const bool ok = mbar_wait(bar_done, 0, abort_flag);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int m = warp * 32 + lane;                 // accumulator row = TMEM lane
+    const int quarter = warp & 3;                    // TMEM lane quarter of this warp
+    const int R = mt * 128 + quarter * 32 + lane;    // plane row of this accumulator row
     const int64_t n = 6 * (int64_t)P;
-    const bool mrow = ok && m < 6 * na;
-    const int a = mt * kTcMBlocks + m / 6, x = m % 6;
+    const bool mrow = ok && R < 6 * nr;
+    const int a = R / 6, x = R % 6;
     const int pa = mrow ? spose[a] : 0;
-    for (int col0 = 0; col0 < Npad; col0 += 16) {
+    for (int col0 = (warp >> 2) * 16; col0 < Npad; col0 += 32) {
       uint32_t v[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col0;
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
           : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
@@ -894,10 +933,42 @@ ba_schur_tc_kernel(int HW, int chunk, BaPtrs w, int P, int32_t* __restrict__ inf
   if (*abort_flag && tid == 0) atomicOr(info, HS2_DEV_TIMEOUT);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 4) {
+  if (warp == kTcSplitWarps) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
   }
+}
+
+// Tensor map over the E planes [6*rows, HW] (row stride row_stride(HW) floats): boxes of
+// 64 plane rows x 32 pixels, 128B swizzle, zero fill past HW.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int encode_erows_map(CUtensorMap* map, float* erows, int HW, int64_t plane_rows) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* f = nullptr;
+    HS2_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !f) {
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return HS2_ERR_CUDA;
+    }
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)HW, (cuuint64_t)plane_rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)row_stride(HW) * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)kTcK, (cuuint32_t)kTcBox};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, erows, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return HS2_ERR_CUDA;
+  }
+  return HS2_OK;
 }
 
 // ------------------------------------------------------------- cholesky ---
@@ -1019,12 +1090,19 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
             colD[p][ty * 4 + a] = vd;
             colX[p][ty * 4 + a] = vx;
             if (ty == (j >> 2) && a == cj) {
-              // pivot owner: reciprocals once per column
-              const double sq = vd > 0.0 ? sqrt(vd) : 0.0;
-              const double sinv = vd > 0.0 ? 1.0 / sq : 0.0;
+              // pivot owner: 1/sqrt(d) from a single-precision seed and two FP64 Newton
+              // steps (23 -> 46 -> full bits), no IEEE divide or sqrt on the critical path
+              double sinv = 0.0;
+              if (vd > 1e-30 && vd < 1e30) {
+                sinv = (double)rsqrtf((float)vd);
+                sinv = sinv * (1.5 - 0.5 * vd * sinv * sinv);
+                sinv = sinv * (1.5 - 0.5 * vd * sinv * sinv);
+              } else if (vd > 0.0) {
+                sinv = 1.0 / sqrt(vd);
+              }
               piv[p][0] = vd;
               piv[p][1] = sinv * sinv;
-              piv[p][2] = sq;
+              piv[p][2] = vd * sinv;
               piv[p][3] = sinv;
             }
           }
@@ -1037,13 +1115,22 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
         }
         const double rinv = piv[p][1], sq = piv[p][2], sinv = piv[p][3];
         const double bjr = sbj[p] * rinv;
-        double cl[4], ci[4], xi[4];
+        // Branch-free update: multipliers of rows/columns at or before the pivot are
+        // zero, so every thread runs the same 32 FMAs; column j is then scaled by selects.
+        double cl[4], ci[4], xi[4], sc[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) cl[c] = colD[p][tx * 4 + c] * rinv;
+        for (int c = 0; c < 4; ++c) {
+          const int l = tx * 4 + c;
+          const double v = colD[p][l] * rinv;
+          cl[c] = l > j ? v : 0.0;
+          sc[c] = l == j ? sinv : 1.0;
+        }
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-          ci[a] = colD[p][ty * 4 + a];
-          xi[a] = colX[p][ty * 4 + a];
+          const int i = ty * 4 + a;
+          const double v = colD[p][i];
+          ci[a] = i > j ? v : 0.0;
+          xi[a] = colX[p][i];
         }
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
@@ -1051,19 +1138,13 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             const int l = tx * 4 + c;
-            if (l > j) {
-              if (i > j) d[a][c] -= ci[a] * cl[c];
-              x[a][c] -= xi[a] * cl[c];
-            } else if (l == j) {
-              d[a][c] = i > j ? d[a][c] * sinv : (i == j ? sq : d[a][c]);
-              x[a][c] *= sinv;
-            }
+            const double dn = fma(-ci[a], cl[c], d[a][c]);
+            d[a][c] = (l == j && i == j) ? sq : (l == j && i < j) ? d[a][c] : dn * sc[c];
+            x[a][c] = fma(-xi[a], cl[c], x[a][c]) * sc[c];
           }
-          if (tx == 0) {
-            if (i > j) bd[a] -= ci[a] * bjr;
-            else if (i == j) bd[a] *= sinv;
-            bx[a] -= xi[a] * bjr;
-          }
+          const double bn = fma(-ci[a], bjr, bd[a]);
+          bd[a] = (tx == 0) ? (i == j ? bd[a] * sinv : bn) : bd[a];
+          bx[a] = (tx == 0) ? fma(-xi[a], bjr, bx[a]) : bx[a];
         }
       }
       if (bad) {
@@ -1078,7 +1159,18 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
           const int l = tx * 4 + c;
           if (t == 0) {
             cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? d[a][c] : 0.0;
-            if (l == i && i < nb) cb.dinv[(int64_t)kb * kNB + i] = 1.0 / d[a][c];
+            if (l == i && i < nb) {
+              const double lv = d[a][c];
+              double r;
+              if (lv > 1e-15 && lv < 1e15) {
+                r = (double)(1.0f / (float)lv);
+                r = r * (2.0 - lv * r);
+                r = r * (2.0 - lv * r);
+              } else {
+                r = 1.0 / lv;
+              }
+              cb.dinv[(int64_t)kb * kNB + i] = r;
+            }
           } else if (i < nr && l < nb) {
             A[(int64_t)(r0 + i) * n + o + l] = x[a][c];
           }
@@ -1240,6 +1332,7 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
   if (s >= info[1] || s >= dz_rows) return;
   const int f = w.kx[s];
   const int r0 = w.rptr[s], r1 = w.rptr[s + 1];
+  const int HWs = row_stride(HW);
   __shared__ float xs[6];
   float acc[kLinPPT];
   int pix[kLinPPT];
@@ -1254,14 +1347,14 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
     __syncthreads();
     if (threadIdx.x < 6) xs[threadIdx.x] = dx[ix * 6 + threadIdx.x];
     __syncthreads();
-    const float* Er = w.erows + ((int64_t)w.rrow[r] * 6) * HW;
+    const float* Er = w.erows + ((int64_t)r * 6) * HWs;
 #pragma unroll
     for (int k = 0; k < kLinPPT; ++k) {
       const int p = pix[k];
       if (p >= HW) continue;
       float d = 0.f;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) d += Er[(int64_t)c * HW + p] * xs[c];
+      for (int c = 0; c < 6; ++c) d += Er[(int64_t)c * HWs + p] * xs[c];
       acc[k] += d;
     }
   }
@@ -1374,7 +1467,7 @@ struct BaLaunch {
 
 // Schur Gram path: 0 = tensor cores (3xTF32) with the SIMT kernel for frames of more
 // than kTcMaxBlocks rows; 1 = SIMT FP32 for every frame.
-static std::atomic<int> g_schur_path{1};
+static std::atomic<int> g_schur_path{0};
 
 static BaLaunch ba_launch_shape(const BaProblem& p) {
   BaLaunch l;
@@ -1439,8 +1532,11 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
         HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
         attr_set[dev] = true;
       }
-      dim3 grid((unsigned)S, (unsigned)((kTcMaxBlocks + kTcMBlocks - 1) / kTcMBlocks), l.tc_split);
-      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(p.HW, l.tc_chunk, w, P, info);
+      CUtensorMap emap;
+      int rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
+      if (rc) return rc;
+      dim3 grid((unsigned)S, (unsigned)((6 * kTcMaxBlocks + 127) / 128), l.tc_split);
+      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info);
       HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
     }
     dim3 grid((unsigned)S, l.schur_split);

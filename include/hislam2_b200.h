@@ -175,10 +175,10 @@ int hs2_ba_reduced_system(const float* poses, int64_t num_poses, const float* di
 
 /* Selects the kernel of the Schur Gram for later hs2_ba calls (process-wide; no
  * counterpart in the reference, whose Gram is SIMT FP32 in EEt6x6_kernel):
- *   0 tensor cores, tcgen05 kind::tf32 with a hi/lo split of both operands
+ *   0 (default) tensor cores, tcgen05 kind::tf32 with a hi/lo split of both operands
  *     (3 products, about FP32 accuracy) -- depth frames with more than 42 Schur rows
- *     fall back to the SIMT kernel;
- *   1 (default) SIMT FP32 for every frame.
+ *     fall back to the SIMT kernel; needs eta > 0 (Q = 1/(C+eta) >= 0);
+ *   1 SIMT FP32 for every frame.
  */
 int hs2_ba_set_schur_path(int path);
 

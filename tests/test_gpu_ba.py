@@ -99,7 +99,7 @@ def schur_path(request):
     from hislam2_b200 import _lib
     _lib.set_schur_path(request.param)
     yield request.param
-    _lib.set_schur_path(1)
+    _lib.set_schur_path(0)
 
 
 @pytest.mark.parametrize("case", list(CASES))
