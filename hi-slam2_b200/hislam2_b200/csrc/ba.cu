@@ -991,6 +991,7 @@ static int encode_erows_map(CUtensorMap* map, float* erows, int HW, int64_t plan
 // reference's solver fallback.  Every spin of the grid barrier is bounded: on
 // timeout the kernel sets HS2_DEV_TIMEOUT and returns.
 constexpr int kCholThreads = 256;
+constexpr int kPLD = 66;   // padded row length of the panel in shared memory
 constexpr unsigned kBarrierSpins = 1u << 22;
 
 struct CholBuf {
@@ -1040,7 +1041,6 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
                    int32_t* __restrict__ info) {
   if (info[0]) return;
   extern __shared__ double csm[];
-  __shared__ double colD[2][kNB], colX[2][kNB], sbj[2], piv[2][4];
   const unsigned G = gridDim.x;
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int nbk = (n + kNB - 1) / kNB;
@@ -1058,127 +1058,139 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
     const int o = kb * kNB;
     const int nb = min(kNB, n - o);
     const int rest = nbk - kb - 1;
-    // ---- panel
+    // ---- panel: left-looking over four 16-column sub-panels of [D; X | b] in shared memory
     for (int t = blockIdx.x; t <= rest; t += G) {
       const int r0 = o + nb + (t - 1) * kNB;
       const int nr = t == 0 ? 0 : min(kNB, n - r0);
-      double d[4][4], x[4][4], bd[4], bx[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = ty * 4 + a;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int l = tx * 4 + c;
-          d[a][c] = (i < nb && l < nb) ? __ldcg(&A[(int64_t)(o + i) * n + o + l]) : 0.0;
-          x[a][c] = (i < nr && l < nb) ? __ldcg(&A[(int64_t)(r0 + i) * n + o + l]) : 0.0;
-        }
-        bd[a] = i < nb ? __ldcg(&bvec[o + i]) : 0.0;
-        bx[a] = i < nr ? __ldcg(&bvec[r0 + i]) : 0.0;
+      double (*Pm)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);   // [128][kPLD]
+      double* bv = csm + 128 * kPLD;                                   // [128]
+      double* sv = bv + 128;                                           // [64] 1/sqrt(pivot)
+      __syncthreads();
+      for (int idx = tid; idx < 128 * (kNB / 2); idx += kCholThreads) {
+        const int r = idx >> 5, k = (idx & 31) * 2;
+        const bool live = r < kNB ? r < nb : r - kNB < nr;
+        const double* src = A + (int64_t)(r < kNB ? o + r : r0 + r - kNB) * n + o + k;
+        double2 v = make_double2(0.0, 0.0);
+        if (live && k + 1 < nb) v = ldcg2(src);          // stays inside the row (n is even)
+        else if (live && k < nb) v.x = __ldcg(src);
+        Pm[r][k] = v.x;
+        Pm[r][k + 1] = v.y;
       }
+      if (tid < 128) {
+        const int r = tid;
+        bv[r] = r < kNB ? (r < nb ? __ldcg(&bvec[o + r]) : 0.0) : (r - kNB < nr ? __ldcg(&bvec[r0 + r - kNB]) : 0.0);
+      }
+      __syncthreads();
+      const int r = tid >> 1, h = tid & 1;     // my row and column half of the sub-panel
+      const bool xrow = r >= kNB;
+      const bool rowlive = xrow ? (r - kNB < nr) : (r < nb);
       bool bad = false;
-      for (int j = 0; j < nb; ++j) {
-        const int p = j & 1;
-        const int cj = j & 3;
-        if (tx == (j >> 2)) {
+      for (int c0 = 0; c0 < nb && !bad; c0 += 16) {
+        const int c1 = min(c0 + 16, nb);
+        // (a) left-looking update of the sub-panel columns (and of b in the sub-panel rows)
+        if (c0 > 0) {
+          if (rowlive && (xrow || r >= c0)) {
+            double acc[8];
 #pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            // select column cj without dynamic register indexing
-            double vd = d[a][0], vx = x[a][0];
-            if (cj == 1) { vd = d[a][1]; vx = x[a][1]; }
-            if (cj == 2) { vd = d[a][2]; vx = x[a][2]; }
-            if (cj == 3) { vd = d[a][3]; vx = x[a][3]; }
-            colD[p][ty * 4 + a] = vd;
-            colX[p][ty * 4 + a] = vx;
-            if (ty == (j >> 2) && a == cj) {
-              // pivot owner: 1/sqrt(d) from a single-precision seed and two FP64 Newton
-              // steps (23 -> 46 -> full bits), no IEEE divide or sqrt on the critical path
-              double sinv = 0.0;
-              if (vd > 1e-30 && vd < 1e30) {
-                sinv = (double)rsqrtf((float)vd);
-                sinv = sinv * (1.5 - 0.5 * vd * sinv * sinv);
-                sinv = sinv * (1.5 - 0.5 * vd * sinv * sinv);
-              } else if (vd > 0.0) {
-                sinv = 1.0 / sqrt(vd);
-              }
-              piv[p][0] = vd;
-              piv[p][1] = sinv * sinv;
-              piv[p][2] = vd * sinv;
-              piv[p][3] = sinv;
+            for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+            for (int k = 0; k < c0; ++k) {
+              const double pr = Pm[r][k];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) acc[q] = fma(pr, Pm[c0 + 8 * h + q][k], acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int l = c0 + 8 * h + q;
+              if (l < c1) Pm[r][l] -= acc[q];
+            }
+            if (h == 0 && !xrow && r < c1) {
+              double bacc = 0.0;
+              for (int k = 0; k < c0; ++k) bacc = fma(Pm[r][k], bv[k], bacc);
+              bv[r] -= bacc;
             }
           }
+          __syncthreads();
         }
-        if (tx == 0 && ty == (j >> 2)) sbj[p] = cj == 0 ? bd[0] : cj == 1 ? bd[1] : cj == 2 ? bd[2] : bd[3];
-        __syncthreads();
-        if (!(piv[p][0] > 0.0)) {
-          bad = true;
-          break;
-        }
-        const double rinv = piv[p][1], sq = piv[p][2], sinv = piv[p][3];
-        const double bjr = sbj[p] * rinv;
-        // Branch-free update: multipliers of rows/columns at or before the pivot are
-        // zero, so every thread runs the same 32 FMAs; column j is then scaled by selects.
-        double cl[4], ci[4], xi[4], sc[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int l = tx * 4 + c;
-          const double v = colD[p][l] * rinv;
-          cl[c] = l > j ? v : 0.0;
-          sc[c] = l == j ? sinv : 1.0;
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int i = ty * 4 + a;
-          const double v = colD[p][i];
-          ci[a] = i > j ? v : 0.0;
-          xi[a] = colX[p][i];
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int i = ty * 4 + a;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int l = tx * 4 + c;
-            const double dn = fma(-ci[a], cl[c], d[a][c]);
-            d[a][c] = (l == j && i == j) ? sq : (l == j && i < j) ? d[a][c] : dn * sc[c];
-            x[a][c] = fma(-xi[a], cl[c], x[a][c]) * sc[c];
+        // (b) column elimination inside the sub-panel; column j is scaled one step later
+        double sinv_prev = 0.0, sq_prev = 0.0;
+        for (int j = c0; j < c1; ++j) {
+          const double dj = Pm[j][j];
+          if (!(dj > 0.0)) {
+            bad = true;
+            break;
           }
-          const double bn = fma(-ci[a], bjr, bd[a]);
-          bd[a] = (tx == 0) ? (i == j ? bd[a] * sinv : bn) : bd[a];
-          bx[a] = (tx == 0) ? fma(-xi[a], bjr, bx[a]) : bx[a];
+          double sinv;
+          if (dj > 1e-30 && dj < 1e30) {
+            sinv = (double)rsqrtf((float)dj);
+            sinv = sinv * (1.5 - 0.5 * dj * sinv * sinv);
+            sinv = sinv * (1.5 - 0.5 * dj * sinv * sinv);
+          } else {
+            sinv = 1.0 / sqrt(dj);
+          }
+          const double rinv = sinv * sinv;
+          const double mr = (rowlive && (xrow || r > j)) ? Pm[r][j] : 0.0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int l = c0 + 8 * h + q;
+            const double ml = (l > j && l < c1) ? Pm[l][j] * rinv : 0.0;
+            if (l > j && l < c1) Pm[r][l] = fma(-mr, ml, Pm[r][l]);
+          }
+          if (h == 0 && !xrow && r > j && r < c1) bv[r] = fma(-mr, bv[j] * rinv, bv[r]);
+          // deferred scaling of column j-1 (not read in this step)
+          if (j > c0) {
+            const int jp = j - 1;
+            if (h == 0) {
+              if (rowlive && (xrow || r > jp)) Pm[r][jp] *= sinv_prev;
+              if (r == jp) {
+                Pm[jp][jp] = sq_prev;
+                bv[jp] *= sinv_prev;
+              }
+            }
+          }
+          if (tid == 0) sv[j] = sinv;
+          sinv_prev = sinv;
+          sq_prev = dj * sinv;
+          __syncthreads();
+        }
+        if (bad) break;
+        {
+          const int jp = c1 - 1;
+          if (h == 0) {
+            if (rowlive && (xrow || r > jp)) Pm[r][jp] *= sinv_prev;
+            if (r == jp) {
+              Pm[jp][jp] = sq_prev;
+              bv[jp] *= sinv_prev;
+            }
+          }
+          __syncthreads();
         }
       }
       if (bad) {
         if (tid == 0) atomicExch(cb.ctl + 2, 1u);
         break;
       }
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int i = ty * 4 + a;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int l = tx * 4 + c;
-          if (t == 0) {
-            cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? d[a][c] : 0.0;
-            if (l == i && i < nb) {
-              const double lv = d[a][c];
-              double r;
-              if (lv > 1e-15 && lv < 1e15) {
-                r = (double)(1.0f / (float)lv);
-                r = r * (2.0 - lv * r);
-                r = r * (2.0 - lv * r);
-              } else {
-                r = 1.0 / lv;
-              }
-              cb.dinv[(int64_t)kb * kNB + i] = r;
-            }
-          } else if (i < nr && l < nb) {
-            A[(int64_t)(r0 + i) * n + o + l] = x[a][c];
-          }
+      // X rows: b2 -= L21 y1 over all nb columns
+      if (xrow && rowlive && h == 0) {
+        double bacc = 0.0;
+        for (int k = 0; k < nb; ++k) bacc = fma(Pm[r][k], bv[k], bacc);
+        bv[r] -= bacc;
+      }
+      __syncthreads();
+      if (t == 0) {
+        for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
+          const int i = idx >> 6, l = idx & 63;
+          cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? Pm[i][l] : 0.0;
         }
-        if (tx == 0) {
-          if (t == 0 && i < nb) cb.y[o + i] = bd[a];
-          if (t != 0 && i < nr) bvec[r0 + i] = bx[a];
+        if (tid < kNB) {
+          cb.dinv[(int64_t)kb * kNB + tid] = tid < nb ? sv[tid] : 0.0;
+          if (tid < nb) cb.y[o + tid] = bv[tid];
         }
+      } else {
+        for (int idx = tid; idx < nr * kNB; idx += kCholThreads) {
+          const int i = idx >> 6, l = idx & 63;
+          if (l < nb) A[(int64_t)(r0 + i) * n + o + l] = Pm[kNB + i][l];
+        }
+        if (tid < nr) bvec[r0 + tid] = bv[kNB + tid];
       }
     }
     if (!grid_barrier(cb.ctl, G, info)) return;
@@ -1440,7 +1452,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   if (n == 0) return HS2_OK;
   HS2_PROF("ba_cholesky", s);
   const int nbk = (n + kNB - 1) / kNB;
-  const size_t smem = sizeof(double) * 2 * kNB * (kNB + 1);
+  const size_t smem = sizeof(double) * std::max(2 * kNB * (kNB + 1), 128 * kPLD + 128 + 64);
   static int grid_cap[64] = {0};
   int dev = 0;
   HS2_CUDA(cudaGetDevice(&dev));
