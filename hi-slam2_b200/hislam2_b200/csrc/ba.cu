@@ -88,7 +88,7 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
   L.L11 = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB * kNB);
   L.dinv = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB);
   L.ychol = take(sizeof(double) * (size_t)(n + 1));
-  L.ctl = take(sizeof(unsigned) * 4);
+  L.ctl = take(sizeof(unsigned) * (4 + (size_t)((n + kNB - 1) / kNB)));   // barrier words + ready flags
   L.total = o;
   return L;
 }
@@ -973,76 +973,464 @@ static int encode_erows_map(CUtensorMap* map, float* erows, int HW, int64_t plan
 
 // ------------------------------------------------------------- cholesky ---
 // Damped FP64 Cholesky factorisation + solve of the reduced camera system in one
-// cooperative (persistent) launch.  Phases are separated by a grid barrier:
+// cooperative (persistent) launch, one CTA per SM:
 //
-//   damping     diag += ep + lm*diag
-//   per 64-wide panel kb
-//     panel     every CTA owning a panel tile eliminates the 64 panel columns of
-//               [D; X | b] (D the diagonal block, redundantly in every such CTA;
-//               X its 64-row tile below; b the right-hand side), register-resident
-//               16x16 threads x 4x4 elements, one __syncthreads per column.  The tile
-//               of D writes L11 and y = L11^-1 b1; the others write L21 and b2 - L21 y1.
-//     syrk      trailing update A22 -= L21 L21^T on the lower 64x64 tiles
-//   backward    per panel from the last: x_kb = L11^-T y_kb, then y_c -= L[kb][c] . x_kb
-//               for every column c left of the panel
+//   damping   diag += ep + lm*diag                                          | barrier
+//   panel 0                                                                 | barrier
+//   for kb = 0 .. nbk-2 (look-ahead by one panel)
+//     A   column block kb+1 -= L[:, kb] L[kb+1, kb]^T in 16-row slices      | barrier
+//     B   panel kb+1 on `rest` CTAs, in parallel with the remaining tiles
+//         of update kb (column blocks kb+2 ..) on the other CTAs             | barrier
+//   backward  x_c = L_cc^-T (y_c - sum_{j>c} L_jc^T x_j), one CTA per block c,
+//             ordered by per-block ready flags instead of grid barriers
 //
-// A non-positive pivot (the matrix is not positive definite) is seen identically
-// by every CTA that factors the panel; the solution is then 0, as in the
-// reference's solver fallback.  Every spin of the grid barrier is bounded: on
-// timeout the kernel sets HS2_DEV_TIMEOUT and returns.
+// Panel kb, task t: the CTA holds [D; X | b] in shared memory (D the 64x64 diagonal
+// block, redundantly in every CTA of the panel; X the t-th 64-row tile below D, none
+// for t == 0; b the right-hand side) and eliminates the 64 columns in four 16-column
+// sub-panels, left-looking: (a) the sub-panel columns receive the updates of the
+// sub-panels left of them, (b) one warp factors the 16x16 diagonal sub-block and
+// its part of b in registers, exchanging columns by shuffles, (c) every row below
+// solves its 16 entries against that sub-block.  Task 0 writes L11, the reciprocal
+// pivots and y = L11^-1 b1; the others write L21 and b2 - L21 y1.
+//
+// A non-positive pivot is seen identically by every CTA that factors the panel; the
+// solution is then 0, as in the reference's solver fallback.  Every spin (grid
+// barrier, ready flag) is bounded: on timeout the kernel sets HS2_DEV_TIMEOUT and
+// returns.  Data written inside the launch is read through L2 (ld.global.cg).
 constexpr int kCholThreads = 256;
-constexpr int kPLD = 66;   // padded row length of the panel in shared memory
+constexpr int kPLD = 66;   // padded row length (doubles) of panel/tile rows in shared memory
 constexpr unsigned kBarrierSpins = 1u << 22;
+constexpr int kCtlFlags = 4;   // ctl[4 + c]: x of block c is final
 
 struct CholBuf {
-  double* L11;      // [nbk][64][64] factored diagonal blocks
+  double* L11;      // [nbk][64][64] factored diagonal blocks (zero above the diagonal)
   double* dinv;     // [nbk][64] reciprocals of their diagonals
   double* y;        // [n] forward-substituted right-hand side
-  unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed
+  unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed, [4 + c] ready flags
 };
 
 __device__ __forceinline__ double2 ldcg2(const double* p) {
   return __ldcg(reinterpret_cast<const double2*>(p));
 }
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
 
+// Sense-free generation barrier over all CTAs of the cooperative launch.  The
+// __syncthreads before thread 0's acq_rel arrival publishes the CTA's writes; the
+// acquire of the new generation + __syncthreads makes the other CTAs' writes visible.
 __device__ __forceinline__ bool grid_barrier(unsigned* ctl, unsigned nblocks, int32_t* info) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen_p = ctl + 1;
-    const unsigned gen = *gen_p;
-    __threadfence();
-    const unsigned arrived = atomicAdd(ctl, 1u) + 1u;
+    const unsigned gen = ld_acquire_gpu(ctl + 1);
     int ok = 1;
-    if (arrived == nblocks) {
-      atomicExch(ctl, 0u);
-      __threadfence();
-      atomicAdd(ctl + 1, 1u);
+    if (atom_add_acq_rel_gpu(ctl, 1u) == nblocks - 1) {
+      st_relaxed_gpu(ctl, 0u);
+      st_release_gpu(ctl + 1, gen + 1);
     } else {
       unsigned spins = 0;
-      while (*gen_p == gen) {
+      while (ld_acquire_gpu(ctl + 1) == gen) {
         if (++spins > kBarrierSpins) {
           ok = 0;
           atomicOr(info, HS2_DEV_TIMEOUT);
           break;
         }
-        __nanosleep(64);
+        if (spins > 64) __nanosleep(32);
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
 }
 
+// Waits (thread 0) until the ready flag is set; false on timeout.
+__device__ __forceinline__ bool wait_flag(const unsigned* f, int32_t* info) {
+  unsigned spins = 0;
+  while (ld_acquire_gpu(f) == 0u) {
+    if (++spins > kBarrierSpins) {
+      atomicOr(info, HS2_DEV_TIMEOUT);
+      return false;
+    }
+    if (spins > 64) __nanosleep(32);
+  }
+  return true;
+}
+
+// (b) One warp factors the nsb x nsb diagonal sub-block at (c0, c0) in registers,
+// fraction-free: step j replaces the trailing entries by (A_rk d_j - A_rj A_kj) 2^-E_j,
+// d_j the pivot and E_j its binary exponent, so no reciprocal sits on the dependency
+// chain from one pivot to the next (the power-of-two scale is exact and keeps the
+// entries in range).  After step j the trailing block equals c_{j+1} times the true
+// Schur complement, c_{j+1} = c_j d_j 2^-E_j, so with s_j = 1/sqrt(c_j d_j):
+//   L_rj = A_rj s_j,   1/L_jj = c_j s_j,   y_j = b_j s_j.
+// Lane = row (0..15) + 16 * column half; a lane holds the 8 entries of its row in its
+// half, padded with the identity outside nsb.  Column j (and b_j) is exchanged
+// through a double-buffered 2 x 20 shared array, one __syncwarp per step.  Writes L
+// (lower part), the multipliers M_rj = L_rj / L_jj above the diagonal (row j), 1/L_jj
+// to sv and y to bv.
+__device__ __forceinline__ void chol_factor_diag(double (*Pm)[kPLD], double* bv, double* sv, double* xc, int c0,
+                                                 int nsb, int* sfail) {
+  const int lane = threadIdx.x & 31, rr = lane & 15, hh = lane >> 4;
+  double a[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int k = 8 * hh + q;
+    a[q] = (rr < nsb && k < nsb) ? Pm[c0 + rr][c0 + k] : (rr == k ? 1.0 : 0.0);
+  }
+  double bb = (hh == 0 && rr < nsb) ? bv[c0 + rr] : 0.0;
+  double cfac = 1.0;
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int hj = j >> 3, qj = j & 7;
+    double* col = xc + (j & 1) * 20;
+    if (hh == hj) col[rr] = a[qj];
+    if (lane == j) col[16] = bb;
+    __syncwarp();
+    const double piv = col[j], colr = col[rr], bj = col[16];
+    double colk[8];
+#pragma unroll
+    for (int q = 0; q < 8; q += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(&col[8 * hh + q]);
+      colk[q] = v.x;
+      colk[q + 1] = v.y;
+    }
+    ok = ok && (piv > 0.0);
+    const long long bits = __double_as_longlong(piv);
+    const double sc = __longlong_as_double((2046LL - ((bits >> 52) & 0x7FF)) << 52);   // 2^-E_j
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (8 * hh + q > j) a[q] = fma(a[q], piv, -(colr * colk[q])) * sc;
+    if (hh == 0 && rr > j) bb = fma(bb, piv, -(colr * bj)) * sc;
+    // column j is final
+    const double cdj = cfac * piv;
+    const double s = rsqrt(cdj);
+    const double linv = cfac * s;
+    cfac = cdj * sc;
+    if (hh == hj && rr >= j && rr < nsb) {
+      const double l = colr * s;
+      Pm[c0 + rr][c0 + j] = l;
+      if (rr > j) Pm[c0 + j][c0 + rr] = l * linv;
+    }
+    if (lane == j && j < nsb) {
+      sv[c0 + j] = linv;
+      bv[c0 + j] = bj * s;
+    }
+  }
+  if (lane == 0 && !ok) *sfail = 1;
+}
+
+// Panel kb, task t (0: D only; t >= 1: D and the (t-1)-th tile below it).  Returns
+// false when a pivot is not positive (ctl[2] is then set).
+__device__ bool chol_panel(int n, int kb, int t, double* __restrict__ A, double* __restrict__ bvec, CholBuf cb,
+                           double* csm) {
+  const int tid = threadIdx.x;
+  const int o = kb * kNB, nb = min(kNB, n - o);
+  const int r0 = o + nb + (t - 1) * kNB;
+  const int nr = t == 0 ? 0 : min(kNB, n - r0);
+  double (*Pm)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);   // [128][kPLD]: D rows, then X rows
+  double* bv = csm + 128 * kPLD;                                   // [128]
+  double* sv = bv + 128;                                           // [64] 1/L_jj
+  double* xc = sv + 64;                                            // [40] column exchange of (b)
+  int* sfail = reinterpret_cast<int*>(xc + 40);
+  __syncthreads();
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    double2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + (half * 8 + q) * kCholThreads;   // double2 index in the 128 x 32 grid
+      const int r = idx >> 5, k = (idx & 31) * 2;
+      const bool live = r < kNB ? r < nb : r - kNB < nr;
+      const double* src = A + (int64_t)(r < kNB ? o + r : r0 + r - kNB) * n + o + k;
+      v[q] = make_double2(0.0, 0.0);
+      if (live && k + 1 < nb) v[q] = ldcg2(src);   // n is even: a pair never leaves the row
+      else if (live && k < nb) v[q].x = __ldcg(src);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + (half * 8 + q) * kCholThreads;
+      *reinterpret_cast<double2*>(&Pm[idx >> 5][(idx & 31) * 2]) = v[q];
+    }
+  }
+  if (tid < 128) {
+    const int r = tid;
+    bv[r] = r < kNB ? (r < nb ? __ldcg(&bvec[o + r]) : 0.0) : (r - kNB < nr ? __ldcg(&bvec[r0 + r - kNB]) : 0.0);
+  }
+  if (tid == 0) *sfail = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < nb; c0 += 16) {
+    const int c1 = min(c0 + 16, nb);
+    if (c0 > 0) {
+      // (a) left-looking update of the sub-panel columns c0 + 2q + h of row r
+      const int r = tid >> 1, h = tid & 1;
+      const bool xrow = r >= kNB;
+      if (xrow ? (r - kNB < nr) : (r >= c0 && r < nb)) {
+        double acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+        for (int k = 0; k < c0; k += 2) {
+          const double2 pr = *reinterpret_cast<const double2*>(&Pm[r][k]);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const double2 pl = *reinterpret_cast<const double2*>(&Pm[c0 + 2 * q + h][k]);
+            acc[q] = fma(pr.x, pl.x, acc[q]);
+            acc[q] = fma(pr.y, pl.y, acc[q]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int l = c0 + 2 * q + h;
+          if (l < c1) Pm[r][l] -= acc[q];
+        }
+        if (h == 0 && !xrow && r < c1) {
+          double b0 = 0.0, b1 = 0.0;
+          for (int k = 0; k < c0; k += 2) {
+            b0 = fma(Pm[r][k], bv[k], b0);
+            b1 = fma(Pm[r][k + 1], bv[k + 1], b1);
+          }
+          bv[r] -= b0 + b1;
+        }
+      }
+      __syncthreads();
+    }
+    // (b)
+    if (tid < 32) chol_factor_diag(Pm, bv, sv, xc, c0, c1 - c0, sfail);
+    __syncthreads();
+    if (*sfail) {
+      if (tid == 0) atomicExch(cb.ctl + 2, 1u);
+      return false;
+    }
+    // (c) rows below the sub-block solve x L_ss^T = v: with u_j = x_j L_jj,
+    // u_j = v_j - sum_{i<j} u_i M_ji (M above the diagonal of the sub-block), x = u / L_jj
+    if (tid < 128) {
+      const int r = tid;
+      if (r >= kNB ? (r - kNB < nr) : (r >= c1 && r < nb)) {
+        double v[16];
+#pragma unroll
+        for (int l = 0; l < 16; ++l) v[l] = c0 + l < c1 ? Pm[r][c0 + l] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 15; ++j) {
+          if (c0 + j < c1) {
+#pragma unroll
+            for (int l = (j + 1) & ~1; l < 16; l += 2) {
+              const double2 m = *reinterpret_cast<const double2*>(&Pm[c0 + j][c0 + l]);
+              if (l > j) v[l] = fma(-v[j], m.x, v[l]);
+              v[l + 1] = fma(-v[j], m.y, v[l + 1]);
+            }
+          }
+        }
+#pragma unroll
+        for (int l = 0; l < 16; ++l)
+          if (c0 + l < c1) Pm[r][c0 + l] = v[l] * sv[c0 + l];
+      }
+    }
+    __syncthreads();
+  }
+  // X rows: b2 -= L21 y1 (four threads per row)
+  {
+    const int i = tid >> 2, part = tid & 3;
+    double s = 0.0;
+    if (i < nr)
+      for (int k = part; k < nb; k += 4) s = fma(Pm[kNB + i][k], bv[k], s);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    __syncthreads();
+    if (i < nr && part == 0) bv[kNB + i] -= s;
+  }
+  __syncthreads();
+  if (t == 0) {
+    for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
+      const int i = idx >> 6, l = idx & 63;
+      cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? Pm[i][l] : 0.0;
+    }
+    if (tid < kNB) {
+      cb.dinv[(int64_t)kb * kNB + tid] = tid < nb ? sv[tid] : 0.0;
+      if (tid < nb) cb.y[o + tid] = bv[tid];
+    }
+  } else {
+    for (int idx = tid; idx < nr * (kNB / 2); idx += kCholThreads) {
+      const int i = idx >> 5, k = (idx & 31) * 2;
+      double* dst = A + (int64_t)(r0 + i) * n + o + k;
+      if (k + 1 < nb) *reinterpret_cast<double2*>(dst) = *reinterpret_cast<const double2*>(&Pm[kNB + i][k]);
+      else if (k < nb) *dst = Pm[kNB + i][k];
+    }
+    if (tid < nr) bvec[r0 + tid] = bv[kNB + tid];
+  }
+  return true;
+}
+
+// A[ri + i][rj + j] -= sum_k L[ri + i][o + k] L[rj + j][o + k] over the 16*RG rows
+// at ri and the 64 columns at rj; `diag` keeps only entries on or below the
+// diagonal of A.  Thread (ty, tx) owns rows ty + 16a and columns tx + 16c.
+template <int RG>
+__device__ void chol_update_tile(int n, double* __restrict__ A, int o, int ri, int rj, bool diag, double* csm) {
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int ni = min(16 * RG, n - ri), nj = min(kNB, n - rj);
+  if (ni <= 0) return;
+  double (*Ai)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);
+  double (*Aj)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm + 64 * kPLD);
+  __syncthreads();
+  {
+    double2 va[RG * 2], vb[8];
+#pragma unroll
+    for (int q = 0; q < RG * 2; ++q) {
+      const int idx = tid + q * kCholThreads;   // double2 index in the (16 RG) x 32 grid
+      const int a = idx >> 5, k = (idx & 31) * 2;
+      va[q] = a < ni ? ldcg2(&A[(int64_t)(ri + a) * n + o + k]) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + q * kCholThreads;
+      const int a = idx >> 5, k = (idx & 31) * 2;
+      vb[q] = a < nj ? ldcg2(&A[(int64_t)(rj + a) * n + o + k]) : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < RG * 2; ++q) {
+      const int idx = tid + q * kCholThreads;
+      *reinterpret_cast<double2*>(&Ai[idx >> 5][(idx & 31) * 2]) = va[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + q * kCholThreads;
+      *reinterpret_cast<double2*>(&Aj[idx >> 5][(idx & 31) * 2]) = vb[q];
+    }
+  }
+  __syncthreads();
+  double acc[RG][4];
+#pragma unroll
+  for (int a = 0; a < RG; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < kNB; k += 2) {
+    double2 va[RG], vb[4];
+#pragma unroll
+    for (int a = 0; a < RG; ++a) va[a] = *reinterpret_cast<const double2*>(&Ai[ty + 16 * a][k]);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) vb[c] = *reinterpret_cast<const double2*>(&Aj[tx + 16 * c][k]);
+#pragma unroll
+    for (int a = 0; a < RG; ++a)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        acc[a][c] = fma(va[a].x, vb[c].x, acc[a][c]);
+        acc[a][c] = fma(va[a].y, vb[c].y, acc[a][c]);
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < RG; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = ty + 16 * a, j = tx + 16 * c;
+      if (i < ni && j < nj && (!diag || rj + j <= ri + i)) {
+        double* dst = &A[(int64_t)(ri + i) * n + rj + j];
+        *dst = __ldcg(dst) - acc[a][c];
+      }
+    }
+}
+
+// Backward substitution L^T x = y, block c on CTA c mod G (blocks taken from the
+// highest down).  The CTA folds L_jc^T x_j into per-thread partial sums as the ready
+// flags of blocks j > c arrive (its loads of L_jc are issued before it waits), then
+// one warp solves with L_cc^T in registers and the block's flag is released.
+__device__ bool chol_backward(int n, int nbk, const double* __restrict__ A, CholBuf cb, double* __restrict__ x,
+                              float* __restrict__ dx_out, int32_t* __restrict__ info, double* csm) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int G = (int)gridDim.x, cta = (int)blockIdx.x;
+  if (cta >= nbk) return true;
+  double (*Ls)[kNB] = reinterpret_cast<double (*)[kNB]>(csm);   // [64][64]
+  double* ys = csm + kNB * kNB;                                   // [64]
+  double* dv = ys + kNB;                                          // [64]
+  double* part = dv + kNB;                                        // [4][64]
+  __shared__ int s_abort;
+  const int cl = tid & 63, rg = tid >> 6;
+  for (int c = cta + ((nbk - 1 - cta) / G) * G; c >= 0; c -= G) {
+    const int oc = c * kNB, nc = min(kNB, n - oc);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + q * kCholThreads;
+      *reinterpret_cast<double2*>(&Ls[idx >> 5][(idx & 31) * 2]) =
+          ldcg2(&cb.L11[((int64_t)c * kNB + (idx >> 5)) * kNB + (idx & 31) * 2]);
+    }
+    if (tid < kNB) {
+      ys[tid] = tid < nc ? __ldcg(&cb.y[oc + tid]) : 0.0;
+      dv[tid] = tid < nc ? __ldcg(&cb.dinv[(int64_t)c * kNB + tid]) : 0.0;
+    }
+    double acc = 0.0;
+    for (int j = nbk - 1; j > c; --j) {
+      const int oj = j * kNB, nj = min(kNB, n - oj);
+      double lv[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int row = rg * 16 + r;
+        lv[r] = (row < nj && cl < nc) ? __ldcg(&A[(int64_t)(oj + row) * n + oc + cl]) : 0.0;
+      }
+      if (tid == 0) s_abort = wait_flag(cb.ctl + kCtlFlags + j, info) ? 0 : 1;
+      __syncthreads();
+      if (s_abort) return false;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int row = rg * 16 + r;
+        const double xv = row < nj ? __ldcg(&x[oj + row]) : 0.0;
+        acc = fma(lv[r], xv, acc);
+      }
+    }
+    part[rg * kNB + cl] = acc;
+    __syncthreads();
+    if (tid < 32) {
+      const unsigned kFull = 0xffffffffu;
+      double y0 = ys[lane] - ((part[lane] + part[kNB + lane]) + (part[2 * kNB + lane] + part[3 * kNB + lane]));
+      const int l1 = lane + 32;
+      double y1 = ys[l1] - ((part[l1] + part[kNB + l1]) + (part[2 * kNB + l1] + part[3 * kNB + l1]));
+#pragma unroll
+      for (int j = kNB - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(kFull, j >= 32 ? y1 : y0, j & 31) * dv[j];
+        if (j >= 32) {
+          if (lane == j - 32) y1 = xj;
+        } else if (lane == j) {
+          y0 = xj;
+        }
+        if (lane < j) y0 = fma(-Ls[j][lane], xj, y0);
+        if (l1 < j) y1 = fma(-Ls[j][l1], xj, y1);
+      }
+      if (lane < nc) {
+        x[oc + lane] = y0;
+        dx_out[oc + lane] = (float)y0;
+      }
+      if (l1 < nc) {
+        x[oc + l1] = y1;
+        dx_out[oc + l1] = (float)y1;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) st_release_gpu(cb.ctl + kCtlFlags + c, 1u);
+  }
+  return true;
+}
+
 __global__ void __launch_bounds__(kCholThreads, 1)
 ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __restrict__ dx_out,
                    int32_t* __restrict__ info) {
   if (info[0]) return;
-  extern __shared__ double csm[];
+  extern __shared__ __align__(16) double csm[];
   const unsigned G = gridDim.x;
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int tid = threadIdx.x;
   const int nbk = (n + kNB - 1) / kNB;
   double* A = w.A;
   double* bvec = w.b;
@@ -1053,286 +1441,49 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
   }
   if (!grid_barrier(cb.ctl, G, info)) return;
 
-  bool failed = false;
-  for (int kb = 0; kb < nbk && !failed; ++kb) {
+  for (int t = blockIdx.x; t < nbk; t += G)
+    if (!chol_panel(n, 0, t, A, bvec, cb, csm)) break;
+  if (!grid_barrier(cb.ctl, G, info)) return;
+  bool failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
+
+  for (int kb = 0; kb + 1 < nbk && !failed; ++kb) {
     const int o = kb * kNB;
-    const int nb = min(kNB, n - o);
     const int rest = nbk - kb - 1;
-    // ---- panel: left-looking over four 16-column sub-panels of [D; X | b] in shared memory
-    for (int t = blockIdx.x; t <= rest; t += G) {
-      const int r0 = o + nb + (t - 1) * kNB;
-      const int nr = t == 0 ? 0 : min(kNB, n - r0);
-      double (*Pm)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);   // [128][kPLD]
-      double* bv = csm + 128 * kPLD;                                   // [128]
-      double* sv = bv + 128;                                           // [64] 1/sqrt(pivot)
-      __syncthreads();
-      for (int idx = tid; idx < 128 * (kNB / 2); idx += kCholThreads) {
-        const int r = idx >> 5, k = (idx & 31) * 2;
-        const bool live = r < kNB ? r < nb : r - kNB < nr;
-        const double* src = A + (int64_t)(r < kNB ? o + r : r0 + r - kNB) * n + o + k;
-        double2 v = make_double2(0.0, 0.0);
-        if (live && k + 1 < nb) v = ldcg2(src);          // stays inside the row (n is even)
-        else if (live && k < nb) v.x = __ldcg(src);
-        Pm[r][k] = v.x;
-        Pm[r][k + 1] = v.y;
-      }
-      if (tid < 128) {
-        const int r = tid;
-        bv[r] = r < kNB ? (r < nb ? __ldcg(&bvec[o + r]) : 0.0) : (r - kNB < nr ? __ldcg(&bvec[r0 + r - kNB]) : 0.0);
-      }
-      __syncthreads();
-      const int r = tid >> 1, h = tid & 1;     // my row and column half of the sub-panel
-      const bool xrow = r >= kNB;
-      const bool rowlive = xrow ? (r - kNB < nr) : (r < nb);
-      bool bad = false;
-      for (int c0 = 0; c0 < nb && !bad; c0 += 16) {
-        const int c1 = min(c0 + 16, nb);
-        // (a) left-looking update of the sub-panel columns (and of b in the sub-panel rows)
-        if (c0 > 0) {
-          if (rowlive && (xrow || r >= c0)) {
-            double acc[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) acc[q] = 0.0;
-            for (int k = 0; k < c0; ++k) {
-              const double pr = Pm[r][k];
-#pragma unroll
-              for (int q = 0; q < 8; ++q) acc[q] = fma(pr, Pm[c0 + 8 * h + q][k], acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int l = c0 + 8 * h + q;
-              if (l < c1) Pm[r][l] -= acc[q];
-            }
-            if (h == 0 && !xrow && r < c1) {
-              double bacc = 0.0;
-              for (int k = 0; k < c0; ++k) bacc = fma(Pm[r][k], bv[k], bacc);
-              bv[r] -= bacc;
-            }
-          }
-          __syncthreads();
-        }
-        // (b) column elimination inside the sub-panel; column j is scaled one step later
-        double sinv_prev = 0.0, sq_prev = 0.0;
-        for (int j = c0; j < c1; ++j) {
-          const double dj = Pm[j][j];
-          if (!(dj > 0.0)) {
-            bad = true;
-            break;
-          }
-          double sinv;
-          if (dj > 1e-30 && dj < 1e30) {
-            sinv = (double)rsqrtf((float)dj);
-            sinv = sinv * (1.5 - 0.5 * dj * sinv * sinv);
-            sinv = sinv * (1.5 - 0.5 * dj * sinv * sinv);
-          } else {
-            sinv = 1.0 / sqrt(dj);
-          }
-          const double rinv = sinv * sinv;
-          const double mr = (rowlive && (xrow || r > j)) ? Pm[r][j] : 0.0;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int l = c0 + 8 * h + q;
-            const double ml = (l > j && l < c1) ? Pm[l][j] * rinv : 0.0;
-            if (l > j && l < c1) Pm[r][l] = fma(-mr, ml, Pm[r][l]);
-          }
-          if (h == 0 && !xrow && r > j && r < c1) bv[r] = fma(-mr, bv[j] * rinv, bv[r]);
-          // deferred scaling of column j-1 (not read in this step)
-          if (j > c0) {
-            const int jp = j - 1;
-            if (h == 0) {
-              if (rowlive && (xrow || r > jp)) Pm[r][jp] *= sinv_prev;
-              if (r == jp) {
-                Pm[jp][jp] = sq_prev;
-                bv[jp] *= sinv_prev;
-              }
-            }
-          }
-          if (tid == 0) sv[j] = sinv;
-          sinv_prev = sinv;
-          sq_prev = dj * sinv;
-          __syncthreads();
-        }
-        if (bad) break;
-        {
-          const int jp = c1 - 1;
-          if (h == 0) {
-            if (rowlive && (xrow || r > jp)) Pm[r][jp] *= sinv_prev;
-            if (r == jp) {
-              Pm[jp][jp] = sq_prev;
-              bv[jp] *= sinv_prev;
-            }
-          }
-          __syncthreads();
-        }
-      }
-      if (bad) {
-        if (tid == 0) atomicExch(cb.ctl + 2, 1u);
-        break;
-      }
-      // X rows: b2 -= L21 y1 over all nb columns
-      if (xrow && rowlive && h == 0) {
-        double bacc = 0.0;
-        for (int k = 0; k < nb; ++k) bacc = fma(Pm[r][k], bv[k], bacc);
-        bv[r] -= bacc;
-      }
-      __syncthreads();
-      if (t == 0) {
-        for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
-          const int i = idx >> 6, l = idx & 63;
-          cb.L11[((int64_t)kb * kNB + i) * kNB + l] = (l <= i && i < nb) ? Pm[i][l] : 0.0;
-        }
-        if (tid < kNB) {
-          cb.dinv[(int64_t)kb * kNB + tid] = tid < nb ? sv[tid] : 0.0;
-          if (tid < nb) cb.y[o + tid] = bv[tid];
-        }
+    // A: column block kb+1, 16-row slices of the tiles below panel kb
+    for (int t = blockIdx.x; t < rest * 4; t += G) {
+      const int I = t >> 2, q = t & 3;
+      chol_update_tile<1>(n, A, o, o + kNB + I * kNB + 16 * q, o + kNB, I == 0, csm);
+    }
+    if (!grid_barrier(cb.ctl, G, info)) return;
+    // B: panel kb+1 (tasks 0..rest-1) || tiles (I, J), 1 <= J <= I < rest, of update kb
+    const int ntiles = rest * (rest - 1) / 2;
+    for (int t = blockIdx.x; t < rest + ntiles; t += G) {
+      if (t < rest) {
+        chol_panel(n, kb + 1, t, A, bvec, cb, csm);
       } else {
-        for (int idx = tid; idx < nr * kNB; idx += kCholThreads) {
-          const int i = idx >> 6, l = idx & 63;
-          if (l < nb) A[(int64_t)(r0 + i) * n + o + l] = Pm[kNB + i][l];
+        int I = 0, tt = t - rest;
+        while (tt > I) {
+          tt -= I + 1;
+          ++I;
         }
-        if (tid < nr) bvec[r0 + tid] = bv[kNB + tid];
+        const int J = tt + 1;
+        ++I;
+        chol_update_tile<4>(n, A, o, o + kNB + I * kNB, o + kNB + J * kNB, I == J, csm);
       }
     }
     if (!grid_barrier(cb.ctl, G, info)) return;
-    if (*(volatile unsigned*)(cb.ctl + 2)) {
-      failed = true;
-      break;
-    }
-    // ---- trailing update
-    const int ntiles = rest * (rest + 1) / 2;
-    double (*Ai)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm);
-    double (*Aj)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm + kNB * (kNB + 1));
-    for (int t = blockIdx.x; t < ntiles; t += G) {
-      int I = 0, tt = t;
-      while (tt > I) { tt -= I + 1; ++I; }
-      const int J = tt;
-      const int ri = o + kNB + I * kNB, rj = o + kNB + J * kNB;
-      const int ni = min(kNB, n - ri), nj = min(kNB, n - rj);
-      __syncthreads();
-      {
-        // 2 x 64x64 doubles, 16 independent loads in flight per thread
-        double2 va[8], vb[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int idx = tid + q * kCholThreads;  // double2 index in the 64x32 grid
-          const int a = idx >> 5, k = (idx & 31) * 2;
-          va[q] = a < ni ? ldcg2(&A[(int64_t)(ri + a) * n + o + k]) : make_double2(0.0, 0.0);
-          vb[q] = a < nj ? ldcg2(&A[(int64_t)(rj + a) * n + o + k]) : make_double2(0.0, 0.0);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int idx = tid + q * kCholThreads;
-          const int a = idx >> 5, k = (idx & 31) * 2;
-          Ai[a][k] = va[q].x; Ai[a][k + 1] = va[q].y;
-          Aj[a][k] = vb[q].x; Aj[a][k + 1] = vb[q].y;
-        }
-      }
-      __syncthreads();
-      double acc[4][4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < kNB; ++k) {
-        double va[4], vb[4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          va[a] = Ai[ty + 16 * a][k];
-          vb[a] = Aj[tx + 16 * a][k];
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) acc[a][c] += va[a] * vb[c];
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int i = ty + 16 * a, j = tx + 16 * c;
-          if (i < ni && j < nj && (I > J || j <= i)) {
-            double* dst = &A[(int64_t)(ri + i) * n + rj + j];
-            *dst = __ldcg(dst) - acc[a][c];
-          }
-        }
-    }
-    if (!grid_barrier(cb.ctl, G, info)) return;
+    failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
   }
 
   if (!failed) {
-    double (*Ls)[kNB + 1] = reinterpret_cast<double (*)[kNB + 1]>(csm);
-    double* ys = csm + kNB * (kNB + 1);
-    double* dv = ys + kNB;
-    double* part = dv + kNB;  // [4][64] partial sums of the update
-    for (int kb = nbk - 1; kb >= 0; --kb) {
-      const int o = kb * kNB;
-      const int nb = min(kNB, n - o);
-      __syncthreads();
-      {
-        double2 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int idx = tid + q * kCholThreads;
-          v[q] = ldcg2(&cb.L11[((int64_t)kb * kNB + (idx >> 5)) * kNB + (idx & 31) * 2]);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int idx = tid + q * kCholThreads;
-          Ls[idx >> 5][(idx & 31) * 2] = v[q].x;
-          Ls[idx >> 5][(idx & 31) * 2 + 1] = v[q].y;
-        }
-      }
-      if (tid < kNB) {
-        ys[tid] = tid < nb ? __ldcg(&cb.y[o + tid]) : 0.0;
-        dv[tid] = tid < nb ? __ldcg(&cb.dinv[(int64_t)kb * kNB + tid]) : 0.0;
-      }
-      __syncthreads();
-      if (tid < 32) {
-        // x = L11^-T y, column-oriented on L11^T (row j of L11)
-        for (int j = nb - 1; j >= 0; --j) {
-          const double xj = ys[j] * dv[j];
-          __syncwarp();
-          if (tid == 0) ys[j] = xj;
-          for (int i = tid; i < j; i += 32) ys[i] -= Ls[j][i] * xj;
-          __syncwarp();
-        }
-      }
-      __syncthreads();
-      if (blockIdx.x == 0)
-        for (int i = tid; i < nb; i += kCholThreads) w.x[o + i] = ys[i];
-      // y_c -= sum_r L[o+r][c] x_r for c < o: 64 columns per CTA, 4 x 16 rows per column
-      const int cl = tid & 63, rg = tid >> 6;
-      for (int c0 = blockIdx.x * kNB; c0 < o; c0 += G * kNB) {
-        const int c = c0 + cl;
-        double sacc = 0.0;
-        if (c < o) {
-          double lv[16];
-#pragma unroll
-          for (int r = 0; r < 16; ++r) {
-            const int row = rg * 16 + r;
-            lv[r] = row < nb ? __ldcg(&A[(int64_t)(o + row) * n + c]) : 0.0;
-          }
-#pragma unroll
-          for (int r = 0; r < 16; ++r) sacc += lv[r] * ys[rg * 16 + r];
-        }
-        part[rg * kNB + cl] = sacc;
-        __syncthreads();
-        if (rg == 0 && c < o) {
-          const double tot = part[cl] + part[kNB + cl] + part[2 * kNB + cl] + part[3 * kNB + cl];
-          cb.y[c] = __ldcg(&cb.y[c]) - tot;
-        }
-        __syncthreads();
-      }
-      if (!grid_barrier(cb.ctl, G, info)) return;
-    }
+    chol_backward(n, nbk, A, cb, w.x, dx_out, info, csm);
+    return;
   }
   for (int i = blockIdx.x * kCholThreads + tid; i < n; i += G * kCholThreads) {
-    const double v = failed ? 0.0 : __ldcg(&w.x[i]);
-    if (failed) w.x[i] = 0.0;
-    dx_out[i] = (float)v;
+    w.x[i] = 0.0;
+    dx_out[i] = 0.0f;
   }
-  if (failed && blockIdx.x == 0 && tid == 0) atomicAdd(&info[2], 1);
+  if (blockIdx.x == 0 && tid == 0) atomicAdd(&info[2], 1);
 }
 
 // -------------------------------------------------------------- backsub ---
@@ -1452,7 +1603,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   if (n == 0) return HS2_OK;
   HS2_PROF("ba_cholesky", s);
   const int nbk = (n + kNB - 1) / kNB;
-  const size_t smem = sizeof(double) * std::max(2 * kNB * (kNB + 1), 128 * kPLD + 128 + 64);
+  const size_t smem = sizeof(double) * (128 * kPLD + 128 + 64 + 40 + 2);   // panel (tile, backward need less)
   static int grid_cap[64] = {0};
   int dev = 0;
   HS2_CUDA(cudaGetDevice(&dev));
@@ -1466,7 +1617,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   }
   const int work = std::max(std::max(nbk, (nbk - 1) * nbk / 2), (n + kCholThreads - 1) / kCholThreads);
   int G = std::max(1, std::min(grid_cap[dev], work));
-  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, 4 * sizeof(unsigned), s));
+  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + nbk) * sizeof(unsigned), s));
   void* args[] = {&n, &lm, &ep, &w, &cb, &dx, &info};
   HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_cholesky_kernel, dim3(G), dim3(kCholThreads), args, smem, s));
   HS2_LAUNCH_CHECK("ba_cholesky_kernel");
