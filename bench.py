@@ -25,7 +25,6 @@ bounded sample of the same workload, and prints the same line with
 """
 
 import argparse
-import datetime
 import json
 import os
 import subprocess
@@ -118,27 +117,21 @@ class Clocks:
 
 # ------------------------------------------------------------ distributed
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1 and args.impl == "ours":
-        torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
-                                             device_id=torch.device("cuda", local))
+    from hislam2_b200 import replicas
+    world, rank, local = replicas.env_ranks()
+    if args.impl == "ours":
+        replicas.init(world, local, backend="nccl", timeout_s=180)
     return world, rank, local
 
 
 def max_over_ranks(x, world, dev):
-    if world == 1:
-        return x
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    from hislam2_b200 import replicas
+    return replicas.max_over_ranks(x, world, dev)
 
 
 def barrier(world):
-    if world > 1:
-        torch.distributed.barrier()
+    from hislam2_b200 import replicas
+    replicas.barrier(world)
 
 
 # ----------------------------------------------------------- algorithmic work
@@ -191,13 +184,13 @@ def roofline(prof, work, steps, iters, peaks, simt, traffic_table):
 # ------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local):
     import droid_backends
-    from hislam2_b200 import _lib, synth
+    from hislam2_b200 import _lib, replicas, synth
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     peaks = measured_peaks()
     simt = _lib.measure_simt_peaks()
-    p = synth.make_ba_problem(WORKLOAD, seed=rank, device=dev)
+    p = synth.make_ba_problem(WORKLOAD, seed=replicas.window_seed(rank), device=dev)
     HW = p["disps"].shape[1] * p["disps"].shape[2]
     init_poses, init_disps = p["poses"].clone(), p["disps"].clone()
     poses, disps = init_poses.clone(), init_disps.clone()
@@ -231,7 +224,7 @@ def run_ours(args, world, rank, local):
     prof = _lib.profile_report(reset=True)
     barrier(world)
     ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
-    value = iters * args.steps * world / (ms / 1e3)
+    value = replicas.throughput(iters * args.steps, ms, world)
 
     # end to end through the public op: pinned host inputs in, updated state out
     host = {k: p[k].cpu().pin_memory() for k in ("poses", "disps", "intrinsics", "targets", "weights", "eta",
@@ -263,7 +256,7 @@ def run_ours(args, world, rank, local):
     e1.record()
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1), world, dev)
-    e2e = {"value": round(iters * args.steps * world / (ms_e2e / 1e3), 3), "unit": UNIT,
+    e2e = {"value": round(replicas.throughput(iters * args.steps, ms_e2e, world), 3), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     corr = corr_lookup(args, dev, world, peaks)
@@ -288,8 +281,7 @@ def run_ours(args, world, rank, local):
                 "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
                 "simt_peaks_tflops": {"fp32": round(simt[0], 2), "fp64": round(simt[1], 2)}}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finalize(world)
 
 
 def corr_lookup(args, dev, world, peaks):
