@@ -107,5 +107,6 @@ def launch_count():
 
 
 def set_schur_path(path):
-    """0: tensor-core Schur Gram (default), 1: SIMT FP32 Schur Gram."""
+    """0: tensor-core Gram over stored E rows (default), 1: SIMT FP32 Gram,
+    2: fused per-frame linearisation + tensor-core Gram."""
     check(load().hs2_ba_set_schur_path(int(path)), "ba_set_schur_path")

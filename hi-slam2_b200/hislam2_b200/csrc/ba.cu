@@ -134,6 +134,44 @@ static BaPtrs ba_ptrs(void* ws, const BaLayout& L) {
 
 // ---------------------------------------------------------------- keys ---
 // In-place exclusive scan of data[0..n) by one CTA of 1024 threads; returns the total.
+// ----------------------------------------------------- frame (fused) ---
+// Linearisation and Schur Gram of a depth frame in one kernel: the E rows never leave
+// shared memory.  One CTA per (depth frame, pixel split), 288 threads:
+//   warps 0-7  per 32-pixel chunk (lane = pixel) warp w linearises edges w, w+8, ... of
+//              the frame: residuals, Jacobians, the edge's Hjj / vj (reduced across the
+//              warp, kept per edge in registers), partial sums of C, w and the frame's
+//              own pose rows, and the E_j rows of Schur edges written raw into the
+//              chunk's K-major 128B-swizzled tile.  Targets and weights of the next two
+//              chunks are in flight meanwhile (cp.async, three stages; each lane copies
+//              and reads only its own values).  After a named barrier of the eight warps
+//              they form Q = 1/(C + eta), scale every tile row by sqrt(Q), add the own
+//              pose rows and the sqrt(Q) w row, and split the tile into TF32 hi/lo parts;
+//   warp 8     allocates TMEM; one lane issues tcgen05.mma kind::tf32 (3xTF32) per chunk
+//              for each 128-row M tile against the whole tile, double-buffered through
+//              mbarriers; at the end warps 0-7 scatter the Gram from TMEM into the FP64
+//              system as ba_schur_tc_kernel does, and each edge's Hjj / vj is added to
+//              its FP64 accumulator.
+// Frames with more than kFMaxEdges edges or kFMaxRows Schur rows are left to the
+// unfused kernels.  Requires Q >= 0 (eta > 0).  Every mbarrier wait is bounded.
+constexpr int kFWarps = 8;
+constexpr int kFThreads = 32 * (kFWarps + 1);
+constexpr int kFK = 32;                                   // pixels per chunk
+constexpr int kFMaxEdges = 40;
+constexpr int kFSlots = kFMaxEdges / kFWarps;             // edges per warp
+constexpr int kFMaxRows = 42;                             // 6 * 42 + 1 <= 256 tile rows
+constexpr int kFLd = 3;                                   // cp.async stages
+constexpr int kFTile = 256 * 128;                         // 256 rows x 32 fp32
+constexpr int kFTiles = 2 * 2 * kFTile;                   // 2 stages x (hi, lo)
+constexpr int kFLdBytes = kFLd * kFWarps * kFSlots * 4 * 32 * 4;
+constexpr int kFRedBytes = 2 * kFWarps * 8 * 32 * 4;
+constexpr int kFTabBytes = kFMaxEdges * kEtab * 4;
+constexpr int kFMetaBytes = 1024;
+constexpr int kFSmem = 1024 + kFTiles + kFLdBytes + kFRedBytes + kFTabBytes + kFMetaBytes;
+
+__device__ __forceinline__ bool frame_fusable(const BaPtrs& w, int s) {
+  return w.gptr[s + 1] - w.gptr[s] <= kFMaxEdges && w.sptr[s + 1] - w.sptr[s] <= kFMaxRows;
+}
+
 __device__ int block_exclusive_scan(int* data, int n, int* sh) {
   int carry = 0;
   for (int base = 0; base < n; base += 1024) {
@@ -317,11 +355,12 @@ __global__ void __launch_bounds__(kLinThreads)
 ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
                     const float* __restrict__ targets, const float* __restrict__ weights,
                     const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj,
-                    int t0, int t1, int motion_only, BaPtrs w, const int32_t* __restrict__ info) {
+                    int t0, int t1, int motion_only, int skip_fusable, BaPtrs w,
+                    const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   const int M = info[1];
-  if (s >= M) return;
+  if (s >= M || (skip_fusable && frame_fusable(w, s))) return;
   const int P = t1 - t0;
   const int HWs = row_stride(HW);
   const int f = w.kx[s];
@@ -539,10 +578,11 @@ __device__ __forceinline__ void schur_scatter_block(double* A, int64_t n, int pa
 }
 
 __global__ void __launch_bounds__(256)
-ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, const int32_t* __restrict__ info) {
+ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, int skip_fusable,
+                const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
-  if (s >= info[1]) return;
+  if (s >= info[1] || (skip_fusable && frame_fusable(w, s))) return;
   const int r0 = w.sptr[s];
   const int nr = w.sptr[s + 1] - r0;
   if (nr == 0 || nr < min_blocks) return;
@@ -936,6 +976,418 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
   if (warp == kTcSplitWarps) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+  }
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// Sum of v[0..31] over the warp's lanes; lane l returns the total of v[l].  Five
+// exchange rounds halve the vector each time (31 shuffles instead of 5 per value).
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16, L = 32; o >= 1; o >>= 1, L >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < L / 2; ++i) {
+      const float send = up ? v[i] : v[i + L / 2];
+      const float keep = up ? v[i + L / 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return v[0];
+}
+
+__global__ void __launch_bounds__(kFThreads, 1)
+ba_frame_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
+                const float* __restrict__ targets, const float* __restrict__ weights,
+                const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj, int t0, int t1,
+                int chunk, BaPtrs w, int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1] || !frame_fusable(w, s)) return;
+  const int c0 = blockIdx.y * chunk;
+  const int c1 = min(HW, c0 + chunk);
+  if (c0 >= c1) return;
+  const int P = t1 - t0;
+  const int f = w.kx[s];
+  const bool inwin = f >= t0 && f < t1;
+  const int g0 = w.gptr[s], ne = w.gptr[s + 1] - g0;
+  const int nr = w.sptr[s + 1] - w.sptr[s];
+  const int rbase = w.rptr[s];
+  const int own = inwin ? w.wpos[f - t0] - rbase : -1;     // Schur row of the frame's own pose
+  const bool gram = nr > 0;
+  const int nrow = 6 * nr;
+  const int Npad = (nrow + 1 + 15) & ~15;
+  const int mtiles = (nrow + 127) / 128;
+  const int nchunks = (c1 - c0 + kFK - 1) / kFK;
+  const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
+
+  extern __shared__ uint8_t f_raw[];
+  const uint32_t raw = smem_u32(f_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* gb = f_raw + (base - raw);
+  uint8_t* tiles = gb;                                                  // [2][hi, lo]
+  float* ldbuf = reinterpret_cast<float*>(gb + kFTiles);               // [kFLd][8][kFSlots][4][32]
+  float* red = reinterpret_cast<float*>(gb + kFTiles + kFLdBytes);     // [2][8][8][32]
+  float* tab = reinterpret_cast<float*>(gb + kFTiles + kFLdBytes + kFRedBytes);   // [kFMaxEdges][48]
+  uint8_t* meta = gb + kFTiles + kFLdBytes + kFRedBytes + kFTabBytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(meta);                  // full[2], empty[2], done
+  int* erow = reinterpret_cast<int*>(meta + 64);                        // [kFMaxEdges] Schur row or -1
+  int* eself = erow + kFMaxEdges;                                       // [kFMaxEdges]
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 512);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 520);
+  const uint32_t bar_full = smem_u32(bars), bar_empty = smem_u32(bars + 2), bar_done = smem_u32(bars + 4);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < ne * kEtab; i += kFThreads) tab[i] = w.etab[(int64_t)w.gedge[g0 + i / kEtab] * kEtab + i % kEtab];
+  if (tid < ne) {
+    const int e = w.gedge[g0 + tid];
+    const int q = w.epos[e] - rbase;
+    erow[tid] = q < nr ? q : -1;
+    eself[tid] = jj[e] == f;
+  }
+  if (tid == 0) {
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(bar_full + 8 * q, kFWarps);
+      mbar_init(bar_empty + 8 * q, 1);
+    }
+    mbar_init(bar_done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kFWarps && gram) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = gram ? *tmem_slot : 0u;
+
+  if (warp < kFWarps) {
+    // ------------------------------------------------------------- linearise
+    const float* Qeta = eta + (eta_rows == 1 ? 0 : (int64_t)s * HW);
+    float hacc[kFSlots];
+#pragma unroll
+    for (int k = 0; k < kFSlots; ++k) hacc[k] = 0.f;
+    float* myld = ldbuf + (warp * kFSlots * 4) * 32 + lane;           // + stage * 8*kFSlots*128, + (k*4+a)*32
+    auto issue = [&](int c) {
+      if (c < nchunks) {
+        const int st = c % kFLd;
+        const int p = c0 + c * kFK + lane;
+        if (p < c1) {
+#pragma unroll
+          for (int k = 0; k < kFSlots; ++k) {
+            const int el = warp + kFWarps * k;
+            if (el < ne) {
+              const int64_t e = w.gedge[g0 + el];
+              const uint32_t dst = smem_u32(myld + st * (kFWarps * kFSlots * 128) + k * 128);
+              cp_async4(dst, targets + e * 2 * HW + p);
+              cp_async4(dst + 128, targets + e * 2 * HW + HW + p);
+              cp_async4(dst + 256, weights + e * 2 * HW + p);
+              cp_async4(dst + 384, weights + e * 2 * HW + HW + p);
+            }
+          }
+        }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    issue(0);
+    issue(1);
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      issue(c + 2);
+      asm volatile("cp.async.wait_group 2;" ::: "memory");
+      const int st = c % kFLd;
+      const int p = c0 + c * kFK + lane;
+      const bool valid = p < c1;
+      const int pc = valid ? p : c1 - 1;
+      const int vi = pc / wd;
+      const float v = (float)vi, u = (float)(pc - vi * wd);
+      const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.f};
+      const float h = disps[(int64_t)f * HW + pc];
+      const int tb = c & 1;
+      uint8_t* thi = tiles + tb * 2 * kFTile;
+      uint8_t* tlo = thi + kFTile;
+      if (gram && c >= 2) ok = ok && mbar_wait(bar_empty + 8 * tb, ((c - 2) >> 1) & 1, abort_flag);
+      float cs = 0.f, ws = 0.f, ei[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < kFSlots; ++k) {
+        const int el = warp + kFWarps * k;
+        if (el >= ne) break;
+        const float* tl = tab + el * kEtab;
+        const float* ld = myld + st * (kFWarps * kFSlots * 128) + k * 128;
+        const float tu = valid ? ld[0] : 0.f, tv = valid ? ld[32] : 0.f;
+        const float wgu = valid ? ld[64] : 0.f, wgv = valid ? ld[96] : 0.f;
+        const float q4[4] = {tl[3], tl[4], tl[5], tl[6]};
+        float Y[3];
+        quat_rotate(q4, X, Y);
+        Y[0] += h * tl[0]; Y[1] += h * tl[1]; Y[2] += h * tl[2];
+        const bool bad = Y[2] < kMinDepth;
+        const float xp = fx * (Y[0] / Y[2]) + cx;
+        const float yp = fy * (Y[1] / Y[2]) + cy;
+        const float z = bad ? 0.f : Y[2];
+        const float dd = bad ? 0.f : 1.f / Y[2];
+        const float d2 = dd * dd;
+        float wu = bad ? 0.f : 0.001f * wgu;
+        float wv = bad ? 0.f : 0.001f * wgv;
+        const float ru = valid ? tu - xp : 0.f;
+        const float rv = valid ? tv - yp : 0.f;
+        const float x = Y[0], y = Y[1];
+        const float Jp0 = fx * dd, Jp2 = fx * (-x * d2);
+        const float Jp4 = fy * dd, Jp5 = fy * (-y * d2);
+        const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y};
+        const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x};
+        const float Jzu = Jp0 * tl[0] + Jp2 * tl[2];
+        const float Jzv = Jp4 * tl[1] + Jp5 * tl[2];
+        cs += wu * Jzu * Jzu + wv * Jzv * Jzv;
+        ws += wu * ru * Jzu + wv * rv * Jzv;
+        if (eself[el]) { wu = 0.f; wv = 0.f; }
+        const float au = wu * ru, av = wv * rv;
+        float H[32];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          const float su = wu * Ju[r], sv = wv * Jv[r];
+#pragma unroll
+          for (int cc = r; cc < 6; ++cc) H[tri6(r, cc)] = su * Ju[cc] + sv * Jv[cc];
+          H[21 + r] = au * Ju[r] + av * Jv[r];
+        }
+#pragma unroll
+        for (int i = 27; i < 32; ++i) H[i] = 0.f;
+        hacc[k] += warp_transpose_sum(H);
+        const float zu = wu * Jzu, zv = wv * Jzv;
+        float Ej[6];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) Ej[r] = zu * Ju[r] + zv * Jv[r];
+        const int q = erow[el];
+        if (gram && q >= 0) {
+#pragma unroll
+          for (int r = 0; r < 6; ++r) *reinterpret_cast<float*>(thi + sw128_off(6 * q + r, lane)) = Ej[r];
+        }
+        if (inwin) {
+#pragma unroll
+          for (int r = 0; r < 6; ++r) {
+            float acc = 0.f;
+#pragma unroll
+            for (int cc = 0; cc < 6; ++cc) acc += tl[8 + r * 6 + cc] * Ej[cc];
+            ei[r] += acc;
+          }
+        }
+      }
+      float* rd = red + tb * (kFWarps * 8 * 32);
+      rd[(warp * 8 + 0) * 32 + lane] = cs;
+      rd[(warp * 8 + 1) * 32 + lane] = ws;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) rd[(warp * 8 + 2 + r) * 32 + lane] = ei[r];
+      asm volatile("bar.sync 1, %0;" ::"r"(kFWarps * 32) : "memory");
+      float ct = 0.f, wt = 0.f;
+#pragma unroll
+      for (int q = 0; q < kFWarps; ++q) {
+        ct += rd[(q * 8 + 0) * 32 + lane];
+        wt += rd[(q * 8 + 1) * 32 + lane];
+      }
+      const float Qp = valid ? 1.0f / (ct + Qeta[pc]) : 0.f;
+      if (warp == 0 && valid) {
+        w.qbuf[(int64_t)s * HW + p] = Qp;
+        w.wbuf[(int64_t)s * HW + p] = wt;
+      }
+      if (gram) {
+        const float sq = sqrtf(fmaxf(Qp, 0.f));
+        for (int r = warp; r < Npad; r += kFWarps) {
+          float g = 0.f;
+          if (r < nrow) {
+            const int a = r / 6;
+            float val;
+            if (a == own) {
+              val = 0.f;
+#pragma unroll
+              for (int q = 0; q < kFWarps; ++q) val += rd[(q * 8 + 2 + (r - 6 * a)) * 32 + lane];
+            } else {
+              val = *reinterpret_cast<const float*>(thi + sw128_off(r, lane));
+            }
+            g = val * sq;
+          } else if (r == nrow) {
+            g = wt * sq;
+          }
+          const uint32_t o = sw128_off(r, lane);
+          const float gh = tf32_hi(g);
+          *reinterpret_cast<float*>(thi + o) = gh;
+          *reinterpret_cast<float*>(tlo + o) = g - gh;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_full + 8 * tb);
+      }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // each edge's Hjj / vj
+#pragma unroll
+    for (int k = 0; k < kFSlots; ++k) {
+      const int el = warp + kFWarps * k;
+      if (el < ne && lane < 27) atomicAdd(&w.hedge[(int64_t)w.gedge[g0 + el] * 27 + lane], (double)hacc[k]);
+    }
+    (void)ok;
+  } else if (gram && lane == 0) {
+    // ------------------------------------------------------------- MMA issuer
+    const uint32_t idesc = umma_idesc_tf32(128, Npad);
+    for (int c = 0; c < nchunks; ++c) {
+      const int tb = c & 1;
+      if (!mbar_wait(bar_full + 8 * tb, (c >> 1) & 1, abort_flag)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t b_hi = base + tb * 2 * kFTile;
+      const uint32_t b_lo = b_hi + kFTile;
+      for (int mt = 0; mt < mtiles; ++mt) {
+        const uint32_t a_hi = b_hi + mt * 128 * 128, a_lo = b_lo + mt * 128 * 128;
+        const uint32_t d = tmem + (uint32_t)(mt * Npad);
+#pragma unroll
+        for (int k = 0; k < kFK / 8; ++k) {
+          const uint32_t kb = k * 32;
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + kb), idesc, (c | k) ? 1u : 0u);
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + kb), idesc, 1u);
+          umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + kb), idesc, 1u);
+        }
+      }
+      umma_commit(bar_empty + 8 * tb);
+    }
+    umma_commit(bar_done);
+  }
+
+  // ------------------------------------------------------------- Gram scatter
+  if (gram && warp < kFWarps) {
+    const bool ok = mbar_wait(bar_done, 0, abort_flag);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int64_t n = 6 * (int64_t)P;
+    const int* spose = w.spose + w.sptr[s];
+    const int quarter = warp & 3;
+    for (int mt = 0; mt < mtiles; ++mt) {
+      const int R = mt * 128 + quarter * 32 + lane;
+      const bool mrow = ok && R < nrow;
+      const int a = R / 6, x = R % 6;
+      const int pa = mrow ? spose[a] : 0;
+      for (int col0 = (warp >> 2) * 16; col0 < Npad; col0 += 32) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * Npad + col0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!mrow) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = col0 + j;
+          const double val = -(double)__uint_as_float(v[j]);
+          if (col < nrow) {
+            const int b = col / 6, y = col % 6;
+            if (b < a) continue;
+            const int pb = spose[b];
+            if (pa > pb) atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], val);
+            else if (pa < pb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], val);
+            else {
+              atomicAdd(&w.A[(pa * 6 + x) * n + pa * 6 + y], val);
+              if (a != b) atomicAdd(&w.A[(pa * 6 + y) * n + pa * 6 + x], val);
+            }
+          } else if (col == nrow) {
+            atomicAdd(&w.b[pa * 6 + x], val);
+          }
+        }
+      }
+    }
+  }
+  if (*abort_flag && tid == 0) atomicOr(info, HS2_DEV_TIMEOUT);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == kFWarps && gram) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+// Back-substitution with the E rows recomputed from the weights (the fused path keeps
+// none): per pixel of depth frame f, dz = Q (w - sum_e E_j(e) . u_e) with
+// u_e = dx_j + L_e^T dx_f, each term present only when its pose index lies in (0, P)
+// as in the reference's EvT6x1 (the frame's own row E_f = sum_e L_e E_j(e)).
+__global__ void __launch_bounds__(kLinThreads)
+ba_backsub_frame_kernel(float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
+                        const float* __restrict__ weights, const int64_t* __restrict__ jj, int t0, int t1,
+                        BaPtrs w, const float* __restrict__ dx, float* __restrict__ dz, int64_t dz_rows,
+                        const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1] || s >= dz_rows) return;
+  const int P = t1 - t0;
+  const int f = w.kx[s];
+  const int fi = f - t0;
+  const bool fdx = fi > 0 && fi < P;
+  const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
+  const int g0 = w.gptr[s], g1 = w.gptr[s + 1];
+  __shared__ float tab[kEtab];
+  __shared__ float uvec[6];
+  int pix[kLinPPT];
+  float dsp[kLinPPT], acc[kLinPPT];
+#pragma unroll
+  for (int k = 0; k < kLinPPT; ++k) {
+    pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
+    dsp[k] = pix[k] < HW ? disps[(int64_t)f * HW + pix[k]] : 0.f;
+    acc[k] = 0.f;
+  }
+  for (int g = g0; g < g1; ++g) {
+    const int e = w.gedge[g];
+    __syncthreads();
+    if (threadIdx.x < kEtab) tab[threadIdx.x] = w.etab[(int64_t)e * kEtab + threadIdx.x];
+    if (threadIdx.x < 6) {
+      const int j = (int)(jj[e] - t0);
+      float u = (j > 0 && j < P) ? dx[j * 6 + threadIdx.x] : 0.f;
+      if (fdx) {
+        const float* L = w.etab + (int64_t)e * kEtab + 8;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) u += L[r * 6 + threadIdx.x] * dx[fi * 6 + r];
+      }
+      uvec[threadIdx.x] = u;
+    }
+    __syncthreads();
+    if (jj[e] == f) continue;   // self edge: E_j = 0
+    const float q4[4] = {tab[3], tab[4], tab[5], tab[6]};
+    const float* wgt = weights + (int64_t)e * 2 * HW;
+#pragma unroll
+    for (int k = 0; k < kLinPPT; ++k) {
+      const int p = pix[k];
+      if (p >= HW) continue;
+      const int vi = p / wd;
+      const float v = (float)vi, u = (float)(p - vi * wd);
+      const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.f};
+      const float h = dsp[k];
+      float Y[3];
+      quat_rotate(q4, X, Y);
+      Y[0] += h * tab[0]; Y[1] += h * tab[1]; Y[2] += h * tab[2];
+      if (Y[2] < kMinDepth) continue;
+      const float z = Y[2], dd = 1.f / Y[2], d2 = dd * dd;
+      const float wu = 0.001f * wgt[p], wv = 0.001f * wgt[HW + p];
+      const float x = Y[0], y = Y[1];
+      const float Jp0 = fx * dd, Jp2 = fx * (-x * d2);
+      const float Jp4 = fy * dd, Jp5 = fy * (-y * d2);
+      const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y};
+      const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x};
+      const float zu = wu * (Jp0 * tab[0] + Jp2 * tab[2]), zv = wv * (Jp4 * tab[1] + Jp5 * tab[2]);
+      float d = 0.f;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) d += (zu * Ju[r] + zv * Jv[r]) * uvec[r];
+      acc[k] += d;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kLinPPT; ++k) {
+    const int p = pix[k];
+    if (p >= HW) continue;
+    const int64_t o = (int64_t)s * HW + p;
+    const float v = w.qbuf[o] * (w.wbuf[o] - acc[k]);
+    dz[o] = v;
+    disps[(int64_t)f * HW + p] += v;
   }
 }
 
@@ -1625,11 +2077,16 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
 }
 
 struct BaLaunch {
-  int nchunk, schur_split, schur_chunk, tc_split, tc_chunk;
+  int nchunk, schur_split, schur_chunk, tc_split, tc_chunk, f_split, f_chunk;
 };
 
-// Schur Gram path: 0 = tensor cores (3xTF32) with the SIMT kernel for frames of more
-// than kTcMaxBlocks rows; 1 = SIMT FP32 for every frame.
+// Linearisation / Schur Gram path:
+//   0  unfused linearisation writing the E rows, tcgen05 Gram over the stored rows
+//      (SIMT above kTcMaxBlocks rows);
+//   1  unfused linearisation, SIMT FP32 Gram for every frame;
+//   2  fused per-frame kernel (E rows stay in shared memory, tcgen05 3xTF32 Gram) for
+//      frames of at most kFMaxEdges edges and kFMaxRows Schur rows, the unfused
+//      linearisation + SIMT Gram for the others, back-substitution recomputing E.
 static std::atomic<int> g_schur_path{0};
 
 static BaLaunch ba_launch_shape(const BaProblem& p) {
@@ -1648,6 +2105,12 @@ static BaLaunch ba_launch_shape(const BaProblem& p) {
   l.tc_chunk = (p.HW + l.tc_split - 1) / l.tc_split;
   l.tc_chunk = (l.tc_chunk + kTcK - 1) / kTcK * kTcK;
   l.tc_split = (p.HW + l.tc_chunk - 1) / l.tc_chunk;
+  // fused split: about 3 waves of one-CTA-per-SM work units, >= 4 chunks of kFK pixels each
+  const int fch = (p.HW + kFK - 1) / kFK;
+  l.f_split = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, fch / 4),
+                                                          (3 * kNumSMs + S - 1) / std::max<int64_t>(S, 1)));
+  l.f_chunk = (fch + l.f_split - 1) / l.f_split * kFK;
+  l.f_split = (p.HW + l.f_chunk - 1) / l.f_chunk;
   return l;
 }
 
@@ -1672,11 +2135,28 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
     HS2_CUDA(cudaMemsetAsync(w.A, 0, sizeof(double) * (size_t)n * n, s));
     HS2_CUDA(cudaMemsetAsync(w.b, 0, sizeof(double) * (size_t)n, s));
   }
+  const int path = g_schur_path.load();
+  const bool fused = !p.motion_only && path == 2;
+  if (fused && S > 0) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    HS2_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !attr_set[dev]) {
+      HS2_CUDA(cudaFuncSetAttribute(ba_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+      attr_set[dev] = true;
+    }
+    dim3 grid((unsigned)S, l.f_split);
+    HS2_PROF("ba_frame", s);
+    ba_frame_kernel<<<grid, kFThreads, kFSmem, s>>>(disps, p.HW, p.wd, intrinsics, targets, weights, eta, eta_rows,
+                                                   jj, p.t0, p.t1, l.f_chunk, w, info);
+    HS2_LAUNCH_CHECK("ba_frame_kernel");
+  }
   if (S > 0) {
     dim3 grid((unsigned)S, l.nchunk);
     HS2_PROF("ba_linearize", s);
     ba_linearize_kernel<<<grid, kLinThreads, 0, s>>>(disps, p.HW, p.wd, intrinsics, targets, weights, eta,
-                                                     eta_rows, jj, p.t0, p.t1, p.motion_only, w, info);
+                                                     eta_rows, jj, p.t0, p.t1, p.motion_only, fused ? 1 : 0, w,
+                                                     info);
     HS2_LAUNCH_CHECK("ba_linearize_kernel");
   }
   if (E > 0 && n > 0) {
@@ -1686,7 +2166,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
   }
   if (!p.motion_only && n > 0 && S > 0) {
     HS2_PROF("ba_schur", s);
-    const bool simt_only = g_schur_path.load() == 1;
+    const bool simt_only = path != 0;
     if (!simt_only) {
       static bool attr_set[64] = {false};
       int dev = 0;
@@ -1703,7 +2183,8 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
       HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
     }
     dim3 grid((unsigned)S, l.schur_split);
-    ba_schur_kernel<<<grid, 256, 0, s>>>(p.HW, l.schur_chunk, w, P, simt_only ? 1 : kTcMaxBlocks + 1, info);
+    ba_schur_kernel<<<grid, 256, 0, s>>>(p.HW, l.schur_chunk, w, P, simt_only ? 1 : kTcMaxBlocks + 1,
+                                         fused ? 1 : 0, info);
     HS2_LAUNCH_CHECK("ba_schur_kernel");
   }
   return HS2_OK;
@@ -1796,8 +2277,14 @@ extern "C" int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num
     if (!p.motion_only && S > 0) {
       dim3 grid((unsigned)S, nchunk);
       HS2_PROF("ba_backsub", s);
-      ba_backsub_kernel<<<grid, kLinThreads, 0, s>>>(disps, p.HW, P, w, dx, dz, dz_rows, info);
-      HS2_LAUNCH_CHECK("ba_backsub_kernel");
+      if (g_schur_path.load() == 2) {
+        ba_backsub_frame_kernel<<<grid, kLinThreads, 0, s>>>(disps, p.HW, p.wd, intrinsics, weights, jj, t0, t1, w,
+                                                             dx, dz, dz_rows, info);
+        HS2_LAUNCH_CHECK("ba_backsub_frame_kernel");
+      } else {
+        ba_backsub_kernel<<<grid, kLinThreads, 0, s>>>(disps, p.HW, P, w, dx, dz, dz_rows, info);
+        HS2_LAUNCH_CHECK("ba_backsub_kernel");
+      }
     }
     if (P > 0) {
       HS2_PROF("ba_pose_retr", s);
@@ -1842,8 +2329,9 @@ extern "C" int hs2_ba_reduced_system(const float* poses, int64_t num_poses, cons
 
 extern "C" int hs2_ba_set_schur_path(int path) {
   using namespace hs2;
-  if (path != 0 && path != 1) {
-    set_error("ba_set_schur_path: path must be 0 (tensor cores) or 1 (SIMT FP32)");
+  if (path < 0 || path > 2) {
+    set_error("ba_set_schur_path: path must be 0 (tensor cores over stored E rows), 1 (SIMT FP32) or 2 (fused, "
+              "tensor cores)");
     return HS2_ERR_INVALID;
   }
   g_schur_path.store(path);

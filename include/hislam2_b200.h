@@ -173,12 +173,17 @@ int hs2_ba_reduced_system(const float* poses, int64_t num_poses, const float* di
                           double* A_out, double* b_out, int32_t* info, void* workspace,
                           size_t workspace_bytes, hs2_stream_t stream);
 
-/* Selects the kernel of the Schur Gram for later hs2_ba calls (process-wide; no
- * counterpart in the reference, whose Gram is SIMT FP32 in EEt6x6_kernel):
- *   0 (default) tensor cores, tcgen05 kind::tf32 with a hi/lo split of both operands
- *     (3 products, about FP32 accuracy) -- depth frames with more than 42 Schur rows
- *     fall back to the SIMT kernel; needs eta > 0 (Q = 1/(C+eta) >= 0);
- *   1 SIMT FP32 for every frame.
+/* Selects the kernels of the linearisation and Schur Gram for later hs2_ba calls
+ * (process-wide; no counterpart in the reference, whose Gram is SIMT FP32 in
+ * EEt6x6_kernel):
+ *   0 (default) linearisation writing the E rows, then their Gram on tensor cores
+ *     (tcgen05 kind::tf32 with a hi/lo split of both operands: 3 products, about FP32
+ *     accuracy); frames with more than 42 Schur rows use the SIMT Gram.  Needs
+ *     eta > 0 (Q = 1/(C+eta) >= 0);
+ *   1 SIMT FP32 Gram for every frame;
+ *   2 one fused kernel per depth frame: linearisation and the tensor-core Gram of its
+ *     E rows straight from shared memory; the back-substitution recomputes E.  Frames
+ *     with more than 40 edges or 42 Schur rows use the unfused kernels.  Needs eta > 0.
  */
 int hs2_ba_set_schur_path(int path);
 

@@ -94,7 +94,7 @@ CASES = {
 }
 
 
-@pytest.fixture(params=[0, 1], ids=["gram_tc", "gram_simt"])
+@pytest.fixture(params=[0, 1, 2], ids=["gram_tc", "gram_simt", "fused"])
 def schur_path(request):
     from hislam2_b200 import _lib
     _lib.set_schur_path(request.param)
