@@ -40,7 +40,7 @@ constexpr int kLinPPT = 4;                          // pixels per thread
 constexpr int kLinChunk = kLinThreads * kLinPPT;    // pixels per CTA
 constexpr int kSchurTP = 32;                        // pixels per smem stage
 constexpr int kNB = 64;                             // blocked Cholesky tile
-constexpr int kEtab = 48;                           // floats per edge in the edge table
+constexpr int kEtab = 56;                           // floats per edge in the edge table
 
 // ------------------------------------------------------------ workspace ---
 struct BaLayout {
@@ -332,6 +332,15 @@ __global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int6
   float* t = etab + (int64_t)e * kEtab;
   t[0] = tij[0]; t[1] = tij[1]; t[2] = tij[2];
   t[3] = qij[0]; t[4] = qij[1]; t[5] = qij[2]; t[6] = qij[3]; t[7] = 0.f;
+  {
+    // rotation matrix of qij (row-major) at 44..52
+    const float x = qij[0], y = qij[1], z = qij[2], ww = qij[3];
+    float* R = t + 44;
+    R[0] = 1.f - 2.f * (y * y + z * z); R[1] = 2.f * (x * y - z * ww);       R[2] = 2.f * (x * z + y * ww);
+    R[3] = 2.f * (x * y + z * ww);       R[4] = 1.f - 2.f * (x * x + z * z); R[5] = 2.f * (y * z - x * ww);
+    R[6] = 2.f * (x * z - y * ww);       R[7] = 2.f * (y * z + x * ww);       R[8] = 1.f - 2.f * (x * x + y * y);
+    for (int k = 53; k < kEtab; ++k) t[k] = 0.f;
+  }
   const double td[3] = {tij[0], tij[1], tij[2]};
   const double qd[4] = {qij[0], qij[1], qij[2], qij[3]};
   double* L64 = etab64 + (int64_t)e * 36;
@@ -351,7 +360,78 @@ __global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int6
 // Upper-triangle order of the 21 entries of a symmetric 6x6 block.
 __device__ __forceinline__ int tri6(int r, int c) { return r * 6 - (r * (r - 1)) / 2 + (c - r); }
 
-__global__ void __launch_bounds__(kLinThreads)
+// Linearisation of one pixel for one edge (reference projective_transform and the
+// per-pixel part of projective_transform_kernel): the point of normalised image
+// coordinates (xn, yn) at disparity h is moved by Gij (tab: t at 0..2, rotation matrix
+// at 44..52) and projected.  Outputs the point Jacobian products of the edge's
+// Hessian block (27 sums: upper triangle of Hjj, then vj) added to H, the Schur
+// terms C (cs) and w (ws), and the row E_j (6).  Pixels closer than kMinDepth
+// contribute nothing but their (zero-weight) residual; a self edge keeps C and w and
+// drops H and E.  The Jacobians have a structural zero each (Ju[1], Jv[0]): those
+// products are never formed.
+__device__ __forceinline__ void lin_pixel(const float* __restrict__ tab, float fx, float fy, float cx, float cy,
+                                          float xn, float yn, float h, float tu, float tv, float wgu, float wgv,
+                                          bool self, float (&H)[32], float& cs, float& ws, float (&Ej)[6]) {
+  const float* R = tab + 44;
+  const float Y0 = fmaf(R[0], xn, fmaf(R[1], yn, R[2])) + h * tab[0];
+  const float Y1 = fmaf(R[3], xn, fmaf(R[4], yn, R[5])) + h * tab[1];
+  const float Y2 = fmaf(R[6], xn, fmaf(R[7], yn, R[8])) + h * tab[2];
+  const bool bad = Y2 < kMinDepth;
+  const float iz = __fdividef(1.0f, Y2);
+  const float xp = fx * (Y0 * iz) + cx;
+  const float yp = fy * (Y1 * iz) + cy;
+  const float z = bad ? 0.f : Y2;
+  const float dd = bad ? 0.f : iz;
+  const float d2 = dd * dd;
+  float wu = bad ? 0.f : 0.001f * wgu;
+  float wv = bad ? 0.f : 0.001f * wgv;
+  const float ru = tu - xp, rv = tv - yp;
+  const float Jp0 = fx * dd, Jp2 = fx * (-Y0 * d2);
+  const float Jp4 = fy * dd, Jp5 = fy * (-Y1 * d2);
+  const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * Y1, Jp0 * z - Jp2 * Y0, -Jp0 * Y1};
+  const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * Y1, -Jp5 * Y0, Jp4 * Y0};
+  const float Jzu = Jp0 * tab[0] + Jp2 * tab[2];
+  const float Jzv = Jp4 * tab[1] + Jp5 * tab[2];
+  cs += wu * Jzu * Jzu + wv * Jzv * Jzv;
+  ws += wu * ru * Jzu + wv * rv * Jzv;
+  if (self) { wu = 0.f; wv = 0.f; }
+  const float au = wu * ru, av = wv * rv;
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const float su = wu * Ju[r], sv = wv * Jv[r];
+#pragma unroll
+    for (int c = r; c < 6; ++c) {
+      if (r != 1 && c != 1) H[tri6(r, c)] = fmaf(su, Ju[c], H[tri6(r, c)]);
+      if (r != 0 && c != 0) H[tri6(r, c)] = fmaf(sv, Jv[c], H[tri6(r, c)]);
+    }
+    if (r != 1) H[21 + r] = fmaf(au, Ju[r], H[21 + r]);
+    if (r != 0) H[21 + r] = fmaf(av, Jv[r], H[21 + r]);
+  }
+  const float zu = wu * Jzu, zv = wv * Jzv;
+  Ej[0] = zu * Ju[0];
+  Ej[1] = zv * Jv[1];
+#pragma unroll
+  for (int r = 2; r < 6; ++r) Ej[r] = fmaf(zu, Ju[r], zv * Jv[r]);
+}
+
+// Sum of v[0..31] over the warp's lanes; lane l returns the total of v[l].  Five
+// exchange rounds halve the vector each time (31 shuffles instead of 5 per value).
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16, L = 32; o >= 1; o >>= 1, L >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < L / 2; ++i) {
+      const float send = up ? v[i] : v[i + L / 2];
+      const float keep = up ? v[i + L / 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return v[0];
+}
+
+__global__ void __launch_bounds__(kLinThreads, 4)
 ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
                     const float* __restrict__ targets, const float* __restrict__ weights,
                     const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj,
@@ -361,21 +441,24 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
   const int s = blockIdx.x;
   const int M = info[1];
   if (s >= M || (skip_fusable && frame_fusable(w, s))) return;
-  const int P = t1 - t0;
   const int HWs = row_stride(HW);
   const int f = w.kx[s];
   const bool inwin = f >= t0 && f < t1;
   const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
 
   __shared__ float tab[kEtab];
-  __shared__ float red[kLinThreads / 32][28];
+  __shared__ float red[kLinThreads / 32][32];
 
   int pix[kLinPPT];
-  float dsp[kLinPPT], Cs[kLinPPT], Ws[kLinPPT], Ei[kLinPPT][6];
+  float dsp[kLinPPT], xn[kLinPPT], yn[kLinPPT], Cs[kLinPPT], Ws[kLinPPT], Ei[kLinPPT][6];
 #pragma unroll
   for (int k = 0; k < kLinPPT; ++k) {
     pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
-    dsp[k] = pix[k] < HW ? disps[(int64_t)f * HW + pix[k]] : 0.f;
+    const int pc = pix[k] < HW ? pix[k] : HW - 1;
+    dsp[k] = disps[(int64_t)f * HW + pc];
+    const int vi = pc / wd;
+    xn[k] = ((float)(pc - vi * wd) - cx) / fx;
+    yn[k] = ((float)vi - cy) / fy;
     Cs[k] = 0.f;
     Ws[k] = 0.f;
 #pragma unroll
@@ -389,69 +472,38 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
     if (threadIdx.x < kEtab) tab[threadIdx.x] = w.etab[(int64_t)e * kEtab + threadIdx.x];
     __syncthreads();
     const bool self = (jj[e] == f);
-    const float t_0 = tab[0], t_1 = tab[1], t_2 = tab[2];
-    const float q[4] = {tab[3], tab[4], tab[5], tab[6]};
     const float* trg = targets + (int64_t)e * 2 * HW;
     const float* wgt = weights + (int64_t)e * 2 * HW;
     float* Erow = w.erows + ((int64_t)w.epos[e] * 6) * HWs;
-
-    float H[27];
+    float tu[kLinPPT], tv[kLinPPT], wgu[kLinPPT], wgv[kLinPPT];
 #pragma unroll
-    for (int k = 0; k < 27; ++k) H[k] = 0.f;
+    for (int k = 0; k < kLinPPT; ++k) {
+      const bool ok = pix[k] < HW;
+      tu[k] = ok ? trg[pix[k]] : 0.f;
+      tv[k] = ok ? trg[HW + pix[k]] : 0.f;
+      wgu[k] = ok ? wgt[pix[k]] : 0.f;
+      wgv[k] = ok ? wgt[HW + pix[k]] : 0.f;
+    }
 
+    float H[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) H[k] = 0.f;
 #pragma unroll
     for (int k = 0; k < kLinPPT; ++k) {
       const int p = pix[k];
       if (p >= HW) continue;
-      const int vi = p / wd;
-      const float v = (float)vi, u = (float)(p - vi * wd);
-      const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.f};
-      const float h = dsp[k];
-      float Y[3];
-      quat_rotate(q, X, Y);
-      Y[0] += h * t_0; Y[1] += h * t_1; Y[2] += h * t_2;
-      const bool bad = Y[2] < kMinDepth;
-      const float xp = fx * (Y[0] / Y[2]) + cx;
-      const float yp = fy * (Y[1] / Y[2]) + cy;
-      const float z = bad ? 0.f : Y[2];
-      const float dd = bad ? 0.f : 1.f / Y[2];
-      const float d2 = dd * dd;
-      float wu = bad ? 0.f : 0.001f * wgt[p];
-      float wv = bad ? 0.f : 0.001f * wgt[HW + p];
-      const float ru = trg[p] - xp;
-      const float rv = trg[HW + p] - yp;
-      const float x = Y[0], y = Y[1];
-      const float Jp0 = fx * dd, Jp2 = fx * (-x * d2);
-      const float Jp4 = fy * dd, Jp5 = fy * (-y * d2);
-      const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y};
-      const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x};
-      const float Jzu = Jp0 * t_0 + Jp2 * t_2;
-      const float Jzv = Jp4 * t_1 + Jp5 * t_2;
-      Cs[k] += wu * Jzu * Jzu + wv * Jzv * Jzv;
-      Ws[k] += wu * ru * Jzu + wv * rv * Jzv;
-      if (self) { wu = 0.f; wv = 0.f; }
-      const float au = wu * ru, av = wv * rv;
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        const float su = wu * Ju[r], sv = wv * Jv[r];
-#pragma unroll
-        for (int c = r; c < 6; ++c) H[tri6(r, c)] += su * Ju[c] + sv * Jv[c];
-        H[21 + r] += au * Ju[r] + av * Jv[r];
-      }
+      float Ej[6];
+      lin_pixel(tab, fx, fy, cx, cy, xn[k], yn[k], dsp[k], tu[k], tv[k], wgu[k], wgv[k], self,
+                H, Cs[k], Ws[k], Ej);
       if (!motion_only) {
-        float Ej[6];
-        const float zu = wu * Jzu, zv = wv * Jzv;
 #pragma unroll
-        for (int r = 0; r < 6; ++r) {
-          Ej[r] = zu * Ju[r] + zv * Jv[r];
-          Erow[(int64_t)r * HWs + p] = Ej[r];
-        }
+        for (int r = 0; r < 6; ++r) Erow[(int64_t)r * HWs + p] = Ej[r];
         if (inwin) {
 #pragma unroll
           for (int r = 0; r < 6; ++r) {
             float acc = 0.f;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) acc += tab[8 + r * 6 + c] * Ej[c];
+            for (int c = 0; c < 6; ++c) acc = fmaf(tab[8 + r * 6 + c], Ej[c], acc);
             Ei[k][r] += acc;
           }
         }
@@ -459,11 +511,7 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
     }
     // block reduction of the 27 Hessian/gradient partial sums of this edge
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 27; ++k) {
-      float v = warp_sum(H[k]);
-      if (lane == 0) red[warp][k] = v;
-    }
+    red[warp][lane] = warp_transpose_sum(H);
     __syncthreads();
     if (threadIdx.x < 27) {
       double acc = 0.0;
@@ -983,23 +1031,6 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
 }
 
-// Sum of v[0..31] over the warp's lanes; lane l returns the total of v[l].  Five
-// exchange rounds halve the vector each time (31 shuffles instead of 5 per value).
-__device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int o = 16, L = 32; o >= 1; o >>= 1, L >>= 1) {
-    const bool up = (lane & o) != 0;
-#pragma unroll
-    for (int i = 0; i < L / 2; ++i) {
-      const float send = up ? v[i] : v[i + L / 2];
-      const float keep = up ? v[i + L / 2] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-    }
-  }
-  return v[0];
-}
-
 __global__ void __launch_bounds__(kFThreads, 1)
 ba_frame_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
                 const float* __restrict__ targets, const float* __restrict__ weights,
@@ -1107,8 +1138,7 @@ ba_frame_kernel(const float* __restrict__ disps, int HW, int wd, const float* __
       const bool valid = p < c1;
       const int pc = valid ? p : c1 - 1;
       const int vi = pc / wd;
-      const float v = (float)vi, u = (float)(pc - vi * wd);
-      const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.f};
+      const float xn = ((float)(pc - vi * wd) - cx) / fx, yn = ((float)vi - cy) / fy;
       const float h = disps[(int64_t)f * HW + pc];
       const int tb = c & 1;
       uint8_t* thi = tiles + tb * 2 * kFTile;
@@ -1123,46 +1153,12 @@ ba_frame_kernel(const float* __restrict__ disps, int HW, int wd, const float* __
         const float* ld = myld + st * (kFWarps * kFSlots * 128) + k * 128;
         const float tu = valid ? ld[0] : 0.f, tv = valid ? ld[32] : 0.f;
         const float wgu = valid ? ld[64] : 0.f, wgv = valid ? ld[96] : 0.f;
-        const float q4[4] = {tl[3], tl[4], tl[5], tl[6]};
-        float Y[3];
-        quat_rotate(q4, X, Y);
-        Y[0] += h * tl[0]; Y[1] += h * tl[1]; Y[2] += h * tl[2];
-        const bool bad = Y[2] < kMinDepth;
-        const float xp = fx * (Y[0] / Y[2]) + cx;
-        const float yp = fy * (Y[1] / Y[2]) + cy;
-        const float z = bad ? 0.f : Y[2];
-        const float dd = bad ? 0.f : 1.f / Y[2];
-        const float d2 = dd * dd;
-        float wu = bad ? 0.f : 0.001f * wgu;
-        float wv = bad ? 0.f : 0.001f * wgv;
-        const float ru = valid ? tu - xp : 0.f;
-        const float rv = valid ? tv - yp : 0.f;
-        const float x = Y[0], y = Y[1];
-        const float Jp0 = fx * dd, Jp2 = fx * (-x * d2);
-        const float Jp4 = fy * dd, Jp5 = fy * (-y * d2);
-        const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y};
-        const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x};
-        const float Jzu = Jp0 * tl[0] + Jp2 * tl[2];
-        const float Jzv = Jp4 * tl[1] + Jp5 * tl[2];
-        cs += wu * Jzu * Jzu + wv * Jzv * Jzv;
-        ws += wu * ru * Jzu + wv * rv * Jzv;
-        if (eself[el]) { wu = 0.f; wv = 0.f; }
-        const float au = wu * ru, av = wv * rv;
         float H[32];
 #pragma unroll
-        for (int r = 0; r < 6; ++r) {
-          const float su = wu * Ju[r], sv = wv * Jv[r];
-#pragma unroll
-          for (int cc = r; cc < 6; ++cc) H[tri6(r, cc)] = su * Ju[cc] + sv * Jv[cc];
-          H[21 + r] = au * Ju[r] + av * Jv[r];
-        }
-#pragma unroll
-        for (int i = 27; i < 32; ++i) H[i] = 0.f;
-        hacc[k] += warp_transpose_sum(H);
-        const float zu = wu * Jzu, zv = wv * Jzv;
+        for (int i = 0; i < 32; ++i) H[i] = 0.f;
         float Ej[6];
-#pragma unroll
-        for (int r = 0; r < 6; ++r) Ej[r] = zu * Ju[r] + zv * Jv[r];
+        lin_pixel(tl, fx, fy, cx, cy, xn, yn, h, tu, tv, wgu, wgv, eself[el] != 0, H, cs, ws, Ej);
+        hacc[k] += warp_transpose_sum(H);
         const int q = erow[el];
         if (gram && q >= 0) {
 #pragma unroll
@@ -1329,11 +1325,15 @@ ba_backsub_frame_kernel(float* __restrict__ disps, int HW, int wd, const float* 
   __shared__ float tab[kEtab];
   __shared__ float uvec[6];
   int pix[kLinPPT];
-  float dsp[kLinPPT], acc[kLinPPT];
+  float dsp[kLinPPT], xn[kLinPPT], yn[kLinPPT], acc[kLinPPT];
 #pragma unroll
   for (int k = 0; k < kLinPPT; ++k) {
     pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
-    dsp[k] = pix[k] < HW ? disps[(int64_t)f * HW + pix[k]] : 0.f;
+    const int pc = pix[k] < HW ? pix[k] : HW - 1;
+    dsp[k] = disps[(int64_t)f * HW + pc];
+    const int vi = pc / wd;
+    xn[k] = ((float)(pc - vi * wd) - cx) / fx;
+    yn[k] = ((float)vi - cy) / fy;
     acc[k] = 0.f;
   }
   for (int g = g0; g < g1; ++g) {
@@ -1352,31 +1352,18 @@ ba_backsub_frame_kernel(float* __restrict__ disps, int HW, int wd, const float* 
     }
     __syncthreads();
     if (jj[e] == f) continue;   // self edge: E_j = 0
-    const float q4[4] = {tab[3], tab[4], tab[5], tab[6]};
     const float* wgt = weights + (int64_t)e * 2 * HW;
 #pragma unroll
     for (int k = 0; k < kLinPPT; ++k) {
       const int p = pix[k];
       if (p >= HW) continue;
-      const int vi = p / wd;
-      const float v = (float)vi, u = (float)(p - vi * wd);
-      const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.f};
-      const float h = dsp[k];
-      float Y[3];
-      quat_rotate(q4, X, Y);
-      Y[0] += h * tab[0]; Y[1] += h * tab[1]; Y[2] += h * tab[2];
-      if (Y[2] < kMinDepth) continue;
-      const float z = Y[2], dd = 1.f / Y[2], d2 = dd * dd;
-      const float wu = 0.001f * wgt[p], wv = 0.001f * wgt[HW + p];
-      const float x = Y[0], y = Y[1];
-      const float Jp0 = fx * dd, Jp2 = fx * (-x * d2);
-      const float Jp4 = fy * dd, Jp5 = fy * (-y * d2);
-      const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y};
-      const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x};
-      const float zu = wu * (Jp0 * tab[0] + Jp2 * tab[2]), zv = wv * (Jp4 * tab[1] + Jp5 * tab[2]);
+      float H[32], cs = 0.f, ws = 0.f, Ej[6];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) H[i] = 0.f;
+      lin_pixel(tab, fx, fy, cx, cy, xn[k], yn[k], dsp[k], 0.f, 0.f, wgt[p], wgt[HW + p], false, H, cs, ws, Ej);
       float d = 0.f;
 #pragma unroll
-      for (int r = 0; r < 6; ++r) d += (zu * Ju[r] + zv * Jv[r]) * uvec[r];
+      for (int r = 0; r < 6; ++r) d = fmaf(Ej[r], uvec[r], d);
       acc[k] += d;
     }
   }
