@@ -758,14 +758,14 @@ __global__ void ba_symmetrize_kernel(int n, double* __restrict__ A) {
 // Tensor-core form of the Schur Gram.  With G = sqrt(Q) o F (the frame's Schur rows
 // scaled per pixel) the frame's block of the Gram is S = G G^T and its rhs column is
 // v = G (sqrt(Q) w): one symmetric GEMM per depth frame with K = pixels, B = [G; sqrt(Q) w]
-// and A = a 128-row window of the same shared-memory tile.  One CTA per (frame, 128-row
-// M tile, pixel split):
+// and A = the one or two 128-row windows of the same shared-memory tile (both held in
+// TMEM, so the tile is loaded and split once).  One CTA per (frame, pixel split):
 //   warp 9     TMA: per 32-pixel chunk, up to four 64x32 fp32 boxes of the frame's E
 //              planes (stored contiguously, depth-frame-major) land 128B-swizzled in
 //              the stage's hi tile (cp.async.bulk.tensor, mbarrier complete_tx);
 //   warps 0-7  scale by sqrt(Q), add the w row, zero the padding and split each value
 //              into TF32 hi/lo parts in place (8 rows in flight per thread);
-//   warp 8     allocates 256 TMEM columns; one lane issues tcgen05.mma kind::tf32
+//   warp 8     allocates 512 TMEM columns; one lane issues tcgen05.mma kind::tf32
 //              M=128, N=Npad, K=8: A_hi.B_hi + A_hi.B_lo + A_lo.B_hi (3xTF32) and
 //              tcgen05.commit releases the stage / finally signals the epilogue;
 //   warps 0-7  read the accumulator (warp w: TMEM lanes of quarter w%4, column half w/4)
@@ -855,8 +855,8 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int nr = w.sptr[s + 1] - w.sptr[s];
-  const int mt = blockIdx.y;
-  if (nr == 0 || nr > kTcMaxBlocks || mt * 128 >= 6 * nr) return;
+  if (nr == 0 || nr > kTcMaxBlocks) return;
+  const int mtiles = (6 * nr + 127) / 128;          // 128-row M tiles, both in this CTA
   const int c0 = blockIdx.z * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
@@ -891,7 +891,7 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
   }
   if (warp == kTcSplitWarps) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(256) : "memory");
+                 "r"(512) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -964,14 +964,17 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t b_hi = base + st * kTcStageBytes;
       const uint32_t b_lo = b_hi + kTcTile;
-      const uint32_t a_hi = b_hi + mt * 128 * 128;
-      const uint32_t a_lo = b_lo + mt * 128 * 128;
+      for (int mt = 0; mt < mtiles; ++mt) {
+        const uint32_t a_hi = b_hi + mt * 128 * 128;
+        const uint32_t a_lo = b_lo + mt * 128 * 128;
+        const uint32_t d = tmem + (uint32_t)(mt * Npad);
 #pragma unroll
-      for (int k = 0; k < kTcK / 8; ++k) {
-        const uint32_t kb = k * 32;
-        umma_tf32(tmem, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + kb), idesc, (c | k) ? 1u : 0u);
-        umma_tf32(tmem, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + kb), idesc, 1u);
-        umma_tf32(tmem, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + kb), idesc, 1u);
+        for (int k = 0; k < kTcK / 8; ++k) {
+          const uint32_t kb = k * 32;
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + kb), idesc, (c | k) ? 1u : 0u);
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + kb), idesc, 1u);
+          umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + kb), idesc, 1u);
+        }
       }
       umma_commit(bar_empty + 8 * st);
     }
@@ -983,37 +986,39 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     const bool ok = mbar_wait(bar_done, 0, abort_flag);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int quarter = warp & 3;                    // TMEM lane quarter of this warp
-    const int R = mt * 128 + quarter * 32 + lane;    // plane row of this accumulator row
     const int64_t n = 6 * (int64_t)P;
-    const bool mrow = ok && R < 6 * nr;
-    const int a = R / 6, x = R % 6;
-    const int pa = mrow ? spose[a] : 0;
-    for (int col0 = (warp >> 2) * 16; col0 < Npad; col0 += 32) {
-      uint32_t v[16];
-      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)col0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (!mrow) continue;
+    for (int mt = 0; mt < mtiles; ++mt) {
+      const int R = mt * 128 + quarter * 32 + lane;  // plane row of this accumulator row
+      const bool mrow = ok && R < 6 * nr;
+      const int a = R / 6, x = R % 6;
+      const int pa = mrow ? spose[a] : 0;
+      for (int col0 = (warp >> 2) * 16; col0 < Npad; col0 += 32) {
+        uint32_t v[16];
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * Npad + col0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (!mrow) continue;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int col = col0 + j;
-        const double val = -(double)__uint_as_float(v[j]);
-        if (col < 6 * nr) {
-          const int b = col / 6, y = col % 6;
-          if (b < a) continue;
-          const int pb = spose[b];
-          if (pa > pb) atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], val);
-          else if (pa < pb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], val);
-          else {
-            atomicAdd(&w.A[(pa * 6 + x) * n + pa * 6 + y], val);
-            if (a != b) atomicAdd(&w.A[(pa * 6 + y) * n + pa * 6 + x], val);
+        for (int j = 0; j < 16; ++j) {
+          const int col = col0 + j;
+          const double val = -(double)__uint_as_float(v[j]);
+          if (col < 6 * nr) {
+            const int b = col / 6, y = col % 6;
+            if (b < a) continue;
+            const int pb = spose[b];
+            if (pa > pb) atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], val);
+            else if (pa < pb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], val);
+            else {
+              atomicAdd(&w.A[(pa * 6 + x) * n + pa * 6 + y], val);
+              if (a != b) atomicAdd(&w.A[(pa * 6 + y) * n + pa * 6 + x], val);
+            }
+          } else if (col == 6 * nr) {
+            atomicAdd(&w.b[pa * 6 + x], val);
           }
-        } else if (col == 6 * nr) {
-          atomicAdd(&w.b[pa * 6 + x], val);
         }
       }
     }
@@ -1023,7 +1028,7 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
   __syncthreads();
   if (warp == kTcSplitWarps) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
 }
 
@@ -1935,7 +1940,8 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
   const int f = w.kx[s];
   const int r0 = w.rptr[s], r1 = w.rptr[s + 1];
   const int HWs = row_stride(HW);
-  __shared__ float xs[6];
+  constexpr int kRows = 64;                 // rows whose dx sit in shared memory at a time
+  __shared__ float xs[kRows][6];
   float acc[kLinPPT];
   int pix[kLinPPT];
 #pragma unroll
@@ -1943,21 +1949,29 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
     pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
     acc[k] = 0.f;
   }
-  for (int r = r0; r < r1; ++r) {
-    const int ix = w.rpose[r];
-    if (ix <= 0 || ix >= P) continue;  // reference EvT6x1_kernel skips ix <= 0
+  for (int rb = r0; rb < r1; rb += kRows) {
+    const int nrw = min(kRows, r1 - rb);
     __syncthreads();
-    if (threadIdx.x < 6) xs[threadIdx.x] = dx[ix * 6 + threadIdx.x];
+    for (int i = threadIdx.x; i < nrw * 6; i += kLinThreads) {
+      const int ix = w.rpose[rb + i / 6];
+      // reference EvT6x1_kernel skips rows of pose index <= 0
+      xs[i / 6][i % 6] = (ix <= 0 || ix >= P) ? 0.f : dx[ix * 6 + i % 6];
+    }
     __syncthreads();
-    const float* Er = w.erows + ((int64_t)r * 6) * HWs;
+#pragma unroll 2
+    for (int i = 0; i < nrw; ++i) {
+      const int ix = w.rpose[rb + i];
+      if (ix <= 0 || ix >= P) continue;
+      const float* Er = w.erows + ((int64_t)(rb + i) * 6) * HWs;
 #pragma unroll
-    for (int k = 0; k < kLinPPT; ++k) {
-      const int p = pix[k];
-      if (p >= HW) continue;
-      float d = 0.f;
+      for (int k = 0; k < kLinPPT; ++k) {
+        const int p = pix[k];
+        if (p >= HW) continue;
+        float d = 0.f;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) d += Er[(int64_t)c * HWs + p] * xs[c];
-      acc[k] += d;
+        for (int c = 0; c < 6; ++c) d = fmaf(__ldcs(&Er[(int64_t)c * HWs + p]), xs[i][c], d);
+        acc[k] += d;
+      }
     }
   }
 #pragma unroll
@@ -2165,7 +2179,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
       CUtensorMap emap;
       int rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
       if (rc) return rc;
-      dim3 grid((unsigned)S, (unsigned)((6 * kTcMaxBlocks + 127) / 128), l.tc_split);
+      dim3 grid((unsigned)S, 1u, l.tc_split);
       ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info);
       HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
     }
