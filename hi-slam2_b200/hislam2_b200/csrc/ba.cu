@@ -771,18 +771,20 @@ __global__ void ba_symmetrize_kernel(int n, double* __restrict__ A) {
 //   warps 0-7  read the accumulator (warp w: TMEM lanes of quarter w%4, column half w/4)
 //              and scatter the a <= b block pairs and the v column into the lower
 //              triangle of the FP64 system.
-// Three stages of 64 KB; every mbarrier wait is bounded (HS2_DEV_TIMEOUT).  Frames with
+// Six stages of 32 KB for frames of at most 128 tile rows, else three of 64 KB; every
+// mbarrier wait is bounded (HS2_DEV_TIMEOUT).  Frames with
 // more than kTcMaxBlocks Schur rows are left to the SIMT kernel.  Requires Q >= 0 (eta > 0).
 constexpr int kTcThreads = 320;
 constexpr int kTcSplitWarps = 8;
 constexpr int kTcK = 32;                       // pixels per stage (128 B per plane row)
-constexpr int kTcStages = 3;
+constexpr int kTcMaxStages = 6;                // stages of frames of <= 128 tile rows
 constexpr int kTcMaxBlocks = 42;               // N <= 6*42 + 1 <= 256
 constexpr int kTcRows = 256;                   // plane rows per tile
 constexpr int kTcBox = 64;                     // plane rows per TMA box
 constexpr int kTcTile = kTcRows * kTcK * 4;    // 32 KB
 constexpr int kTcStageBytes = 2 * kTcTile;     // hi + lo
-constexpr int kTcSmem = kTcStages * kTcStageBytes + 1024 /*align*/ + 2048 /*barriers*/;
+constexpr int kTcArea = 3 * kTcStageBytes;      // 192 KB: 3 stages of 256 rows or 6 of 128
+constexpr int kTcSmem = kTcArea + 1024 /*align*/ + 2048 /*barriers*/;
 constexpr unsigned kTcSpin = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -870,17 +872,21 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
   const uint32_t raw = smem_u32(tc_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* gbase = tc_raw + (base - raw);
-  uint8_t* meta = gbase + kTcStages * kTcStageBytes;
+  uint8_t* meta = gbase + kTcArea;
   uint64_t* bars = reinterpret_cast<uint64_t*>(meta);  // tma[3], full[3], empty[3], done
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 128);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 136);
-  const uint32_t bar_tma = smem_u32(bars), bar_full = smem_u32(bars + 3), bar_empty = smem_u32(bars + 6);
-  const uint32_t bar_done = smem_u32(bars + 9);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(meta + 256);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(meta + 264);
+  const uint32_t bar_tma = smem_u32(bars), bar_full = smem_u32(bars + kTcMaxStages);
+  const uint32_t bar_empty = smem_u32(bars + 2 * kTcMaxStages), bar_done = smem_u32(bars + 3 * kTcMaxStages);
+  // tile rows: 128 when the frame's rows fit (twice the stages in flight), else 256
+  const int trows = Npad <= 128 ? 128 : kTcRows;
+  const uint32_t tile_bytes = (uint32_t)trows * 128u, stage_bytes = 2u * tile_bytes;
+  const int nst = kTcArea / (int)stage_bytes;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int* spose = w.spose + w.sptr[s];
   if (tid == 0) {
-    for (int q = 0; q < kTcStages; ++q) {
+    for (int q = 0; q < nst; ++q) {
       mbar_init(bar_tma + 8 * q, 1);
       mbar_init(bar_full + 8 * q, kTcSplitWarps);
       mbar_init(bar_empty + 8 * q, 1);
@@ -906,11 +912,11 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     if (lane == 0) {
       const uint32_t bytes = (uint32_t)nbox * kTcBox * kTcK * 4;
       for (int c = 0; c < nchunks; ++c) {
-        const int st = c % kTcStages;
-        const int use = c / kTcStages;
+        const int st = c % nst;
+        const int use = c / nst;
         if (use > 0 && !mbar_wait(bar_empty + 8 * st, (use - 1) & 1, abort_flag)) break;
         mbar_arrive_tx(bar_tma + 8 * st, bytes);
-        const uint32_t dst = base + st * kTcStageBytes;
+        const uint32_t dst = base + st * stage_bytes;
         for (int i = 0; i < nbox; ++i)
           tma_load_2d(dst + i * kTcBox * 128, &emap, c0 + c * kTcK, prow0 + i * kTcBox, bar_tma + 8 * st);
       }
@@ -920,16 +926,16 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     int pn = c0 + lane;
     float qn = pn < c1 ? Q[pn] : 0.f, wn = pn < c1 ? Wv[pn] : 0.f;
     for (int c = 0; c < nchunks; ++c) {
-      const int st = c % kTcStages;
+      const int st = c % nst;
       const float sq = sqrtf(fmaxf(qn, 0.f));
       const float wq = wn * sq;
       // prefetch Q, w of the next chunk
       pn = c0 + (c + 1) * kTcK + lane;
       qn = pn < c1 ? Q[pn] : 0.f;
       wn = pn < c1 ? Wv[pn] : 0.f;
-      if (!mbar_wait(bar_tma + 8 * st, (c / kTcStages) & 1, abort_flag)) break;
-      uint8_t* hi = gbase + st * kTcStageBytes;
-      uint8_t* lo = hi + kTcTile;
+      if (!mbar_wait(bar_tma + 8 * st, (c / nst) & 1, abort_flag)) break;
+      uint8_t* hi = gbase + st * stage_bytes;
+      uint8_t* lo = hi + tile_bytes;
       for (int rb = warp; rb < Npad; rb += 8 * kTcSplitWarps) {
         float g[8];
 #pragma unroll
@@ -959,11 +965,11 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     // ------------------------------------------------------------- MMA issuer
     const uint32_t idesc = umma_idesc_tf32(128, Npad);
     for (int c = 0; c < nchunks; ++c) {
-      const int st = c % kTcStages;
-      if (!mbar_wait(bar_full + 8 * st, (c / kTcStages) & 1, abort_flag)) break;
+      const int st = c % nst;
+      if (!mbar_wait(bar_full + 8 * st, (c / nst) & 1, abort_flag)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t b_hi = base + st * kTcStageBytes;
-      const uint32_t b_lo = b_hi + kTcTile;
+      const uint32_t b_hi = base + st * stage_bytes;
+      const uint32_t b_lo = b_hi + tile_bytes;
       for (int mt = 0; mt < mtiles; ++mt) {
         const uint32_t a_hi = b_hi + mt * 128 * 128;
         const uint32_t a_lo = b_lo + mt * 128 * 128;
