@@ -1905,21 +1905,27 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
       chol_update_tile<1>(n, A, o, o + kNB + I * kNB + 16 * q, o + kNB, I == 0, csm);
     }
     if (!grid_barrier(cb.ctl, G, info)) return;
-    // B: panel kb+1 (tasks 0..rest-1) || tiles (I, J), 1 <= J <= I < rest, of update kb
+    // B: panel kb+1 (tasks 0..rest-1) || tiles (I, J), 1 <= J <= I < rest, of update kb.
+    // The panel tasks sit on CTAs of their own (they are the longer tasks); the tiles go
+    // round-robin over the remaining CTAs.
     const int ntiles = rest * (rest - 1) / 2;
-    for (int t = blockIdx.x; t < rest + ntiles; t += G) {
-      if (t < rest) {
+    const bool split = (int)G > rest;
+    const int tfirst = split ? ((int)blockIdx.x < rest ? ntiles : (int)blockIdx.x - rest) : (int)blockIdx.x;
+    const int tstep = split ? (int)G - rest : (int)G;
+    if (split && (int)blockIdx.x < rest) chol_panel(n, kb + 1, blockIdx.x, A, bvec, cb, csm);
+    for (int t = tfirst; t < (split ? ntiles : rest + ntiles); t += tstep) {
+      if (!split && t < rest) {
         chol_panel(n, kb + 1, t, A, bvec, cb, csm);
-      } else {
-        int I = 0, tt = t - rest;
-        while (tt > I) {
-          tt -= I + 1;
-          ++I;
-        }
-        const int J = tt + 1;
-        ++I;
-        chol_update_tile<4>(n, A, o, o + kNB + I * kNB, o + kNB + J * kNB, I == J, csm);
+        continue;
       }
+      int I = 0, tt = split ? t : t - rest;
+      while (tt > I) {
+        tt -= I + 1;
+        ++I;
+      }
+      const int J = tt + 1;
+      ++I;
+      chol_update_tile<4>(n, A, o, o + kNB + I * kNB, o + kNB + J * kNB, I == J, csm);
     }
     if (!grid_barrier(cb.ctl, G, info)) return;
     failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
