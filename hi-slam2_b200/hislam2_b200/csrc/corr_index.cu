@@ -103,6 +103,75 @@ corr_index_fwd_kernel(const T* __restrict__ volume, const float* __restrict__ co
   }
 }
 
+// Forward for a compile-time radius (the network's r = 3 and the r = 4 of the lookup
+// benchmarks): 64 source pixels per CTA; their window origins and fractions are
+// staged first, then every warp gathers the (2R+2)^2 windows of 8 pixels with all its
+// loads issued back to back (tap index -> (row, column) by constant division), and
+// the (2R+1)^2 outputs are formed four threads per pixel, stores contiguous along
+// the pixels.
+template <typename T, int R>
+__global__ void __launch_bounds__(kCiThreads)
+corr_index_fwd_r_kernel(const T* __restrict__ volume, const float* __restrict__ coords, T* __restrict__ corr,
+                        int h1, int w1, int h2, int w2) {
+  constexpr int D = 2 * R + 2, DD = D * D, RD = 2 * R + 1, NOUT = RD * RD;
+  constexpr int TP = 64, STRIDE = (DD & 1) ? DD : DD + 1;
+  constexpr int NT = (DD + 31) / 32;
+  __shared__ float win[TP * STRIDE];
+  __shared__ float2 frac[TP];
+  __shared__ int2 org[TP];
+  const int n = blockIdx.y;
+  const int HW1 = h1 * w1;
+  const int64_t HW2 = (int64_t)h2 * w2;
+  const int pix0 = blockIdx.x * TP;
+  if (threadIdx.x < TP) {
+    const int pix = min(pix0 + (int)threadIdx.x, HW1 - 1);
+    const float cx = coords[((int64_t)n * 2 + 0) * HW1 + pix];
+    const float cy = coords[((int64_t)n * 2 + 1) * HW1 + pix];
+    const float fx = floorf(cx), fy = floorf(cy);
+    frac[threadIdx.x] = make_float2(cx - fx, cy - fy);
+    org[threadIdx.x] = make_int2((int)fx - R, (int)fy - R);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 2
+  for (int q = 0; q < TP / 8; ++q) {
+    const int p = warp * (TP / 8) + q;
+    const int pix = min(pix0 + p, HW1 - 1);
+    const int2 o = org[p];
+    const T* plane = volume + ((int64_t)n * HW1 + pix) * HW2;
+    float v[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      const int t = lane + 32 * k;
+      const int jy = t / D, ix = t - (t / D) * D;
+      const int x1 = o.x + ix, y1 = o.y + jy;
+      v[k] = 0.f;
+      if (t < DD && x1 >= 0 && x1 < w2 && y1 >= 0 && y1 < h2) v[k] = to_f(plane[(int64_t)y1 * w2 + x1]);
+    }
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      const int t = lane + 32 * k;
+      if (t < DD) win[p * STRIDE + t] = v[k];
+    }
+  }
+  __syncthreads();
+  const int p = threadIdx.x & (TP - 1), og = threadIdx.x >> 6;
+  const int pix = pix0 + p;
+  if (pix >= HW1) return;
+  const float2 f = frac[p];
+  const float* w = win + p * STRIDE;
+  T* out = corr + (int64_t)n * NOUT * HW1 + pix;
+#pragma unroll 3
+  for (int o = og; o < NOUT; o += kCiThreads / TP) {
+    const int a = o / RD, b = o - (o / RD) * RD;   // a along x, b along y
+    const float v00 = w[b * D + a], v01 = w[(b + 1) * D + a];
+    const float v10 = w[b * D + a + 1], v11 = w[(b + 1) * D + a + 1];
+    const float val = (1.f - f.x) * (1.f - f.y) * v00 + (1.f - f.x) * f.y * v01 +
+                      f.x * (1.f - f.y) * v10 + f.x * f.y * v11;
+    out[(int64_t)o * HW1] = from_f<T>(val);
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kCiThreads)
 corr_index_bwd_kernel(const float* __restrict__ coords, const T* __restrict__ corr_grad,
@@ -178,8 +247,20 @@ corr_index_bwd_kernel(const float* __restrict__ coords, const T* __restrict__ co
 template <typename T>
 static int launch_fwd(const void* volume, int64_t n, int h1, int w1, int h2, int w2, const float* coords,
                       int radius, void* corr, cudaStream_t stream) {
-  const CiTile t = ci_tile(radius, 2 * radius + 1);
   const int HW1 = h1 * w1;
+  if (radius == 3 || radius == 4) {
+    dim3 grid((HW1 + 63) / 64, (unsigned)n);
+    HS2_PROF("corr_index_fwd", stream);
+    if (radius == 3)
+      corr_index_fwd_r_kernel<T, 3><<<grid, kCiThreads, 0, stream>>>(static_cast<const T*>(volume), coords,
+                                                                      static_cast<T*>(corr), h1, w1, h2, w2);
+    else
+      corr_index_fwd_r_kernel<T, 4><<<grid, kCiThreads, 0, stream>>>(static_cast<const T*>(volume), coords,
+                                                                      static_cast<T*>(corr), h1, w1, h2, w2);
+    HS2_LAUNCH_CHECK("corr_index_fwd_r_kernel");
+    return HS2_OK;
+  }
+  const CiTile t = ci_tile(radius, 2 * radius + 1);
   dim3 grid((HW1 + t.tpix - 1) / t.tpix, (unsigned)n);
   if (t.smem > 48 * 1024)
     HS2_CUDA(cudaFuncSetAttribute(corr_index_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
