@@ -3,16 +3,16 @@
 Exposes the operators of the dense-BA + correlation path with the reference's
 names and positional signatures (``src/droid.cpp:325-341``): ``ba``,
 ``frame_distance``, ``corr_index_forward``, ``corr_index_backward``,
-``altcorr_forward`` and ``altcorr_backward``.  They run on the B200 kernels of
-``hislam2_b200``; there is no CPU fallback.
+``altcorr_forward`` and ``altcorr_backward``, plus the keyframe / point-cloud
+helpers ``covis_distance``, ``depth_filter`` and ``iproj``.  They run on the B200
+kernels of ``hislam2_b200``; there is no CPU fallback.
 
-The reference's other entry points (``pgba``, ``proj_trans``, ``covis_distance``,
-``depth_filter``, ``iproj``, ``bi_inter``) are not part of this path; calling
-them raises ``NotImplementedError`` naming the operator.
+The reference's remaining entry points (``pgba``, ``proj_trans``, ``bi_inter``)
+are not built; calling them raises ``NotImplementedError`` naming the operator.
 """
 
 from hislam2_b200.backends import (ba, frame_distance, corr_index_forward, corr_index_backward,  # noqa: F401
-                                   altcorr_forward, altcorr_backward)
+                                   altcorr_forward, altcorr_backward, covis_distance, depth_filter, iproj)
 
 
 def _not_on_this_path(name):
@@ -25,7 +25,4 @@ def _not_on_this_path(name):
 
 pgba = _not_on_this_path("pgba")
 proj_trans = _not_on_this_path("proj_trans")
-covis_distance = _not_on_this_path("covis_distance")
-depth_filter = _not_on_this_path("depth_filter")
-iproj = _not_on_this_path("iproj")
 bi_inter = _not_on_this_path("bi_inter")

@@ -214,6 +214,68 @@ def frame_distance(poses, disps, intrinsics, ii, jj, beta):
     return dist
 
 
+# ------------------------------------------------------ iproj / covis / depth_filter
+def _geo_inputs(op, poses, disps, intrinsics, extra=()):
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics)) + tuple(extra):
+        _contig(name, t)
+    dev = poses.device
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics)) + tuple(extra):
+        _cuda(name, t, dev)
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics)):
+        _dtype(name, t, torch.float32)
+    if poses.dim() != 2 or poses.shape[1] != 7 or disps.dim() != 3:
+        raise RuntimeError("%s: poses must be [N,7] and disps [N,H,W]" % op)
+    return dev
+
+
+def iproj(poses, disps, intrinsics):
+    """``droid_backends.iproj`` (reference ``src/droid.cpp:233-242``) -> points [N,H,W,3]: every
+    pixel of every disparity frame b back-projected and moved by poses[b]."""
+    dev = _geo_inputs("iproj", poses, disps, intrinsics)
+    N, H, W = disps.shape
+    points = torch.zeros((N, H, W, 3), dtype=torch.float32, device=dev)
+    _lib.check(_lib.load().hs2_iproj(_ptr(poses), poses.shape[0], _ptr(disps), N, H, W, _ptr(intrinsics),
+                                     _ptr(points), _stream(dev)), "iproj")
+    return points
+
+
+def covis_distance(poses, disps, intrinsics, ii):
+    """``droid_backends.covis_distance`` (reference ``src/droid.cpp:218-231``) -> dist [N]: for
+    i = ii[n], the fraction of frame i's pixels outside the image under both neighbours i-1, i+1."""
+    dev = _geo_inputs("covis_distance", poses, disps, intrinsics, (("ii", ii),))
+    _dtype("ii", ii, torch.int64)
+    n = ii.numel()
+    dist = torch.zeros(n, dtype=torch.float32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_covis_distance(_ptr(poses), poses.shape[0], _ptr(disps), disps.shape[0],
+                                              disps.shape[1], disps.shape[2], _ptr(intrinsics), _ptr(ii), n,
+                                              _ptr(dist), _ptr(info), _stream(dev)), "covis_distance")
+    if n and int(info.item()) & _lib.HS2_DEV_BAD_INDEX:
+        raise RuntimeError("covis_distance: every ii must have both neighbours ii-1 and ii+1 in the buffers")
+    return dist
+
+
+def depth_filter(poses, disps, intrinsics, ix, thresh):
+    """``droid_backends.depth_filter`` (reference ``src/droid.cpp:308-322``) -> counter [N,H,W]:
+    per pixel of frame ix[b], how many of the neighbours ix-1, ix-2, ix-3, ix+3, ix+4, ix+5
+    agree with its depth to within thresh[b] (reprojected inverse depth)."""
+    dev = _geo_inputs("depth_filter", poses, disps, intrinsics, (("ix", ix), ("thresh", thresh)))
+    _dtype("ix", ix, torch.int64)
+    _dtype("thresh", thresh, torch.float32)
+    n = ix.numel()
+    if thresh.numel() < n:
+        raise RuntimeError("depth_filter: thresh needs one value per ix entry")
+    N, H, W = disps.shape
+    counter = torch.empty((n, H, W), dtype=torch.float32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_depth_filter(_ptr(poses), poses.shape[0], _ptr(disps), N, H, W, _ptr(intrinsics),
+                                            _ptr(ix), _ptr(thresh), n, _ptr(counter), _ptr(info), _stream(dev)),
+               "depth_filter")
+    if n and int(info.item()) & _lib.HS2_DEV_BAD_INDEX:
+        raise RuntimeError("depth_filter: ix outside the disparity buffer")
+    return counter
+
+
 # ------------------------------------------------------------------ corr_index
 def _corr_dtype(name, t):
     if t.dtype not in _DTYPES:

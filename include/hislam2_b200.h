@@ -173,6 +173,33 @@ int hs2_ba_reduced_system(const float* poses, int64_t num_poses, const float* di
                           double* A_out, double* b_out, int32_t* info, void* workspace,
                           size_t workspace_bytes, hs2_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * iproj  (reference: src/droid.cpp:233-242, src/droid_kernels.cu:1208-1272,2120-2143)
+ * points[b,i,j,:] = (R_b X + d t_b) / d with X = ((j-cx)/fx, (i-cy)/fy, 1), d = disps[b,i,j],
+ * for every frame b of disps (poses must have at least num_disps rows).  points: [N,H,W,3] f32.
+ */
+int hs2_iproj(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht, int wd,
+              const float* intrinsics, float* points, hs2_stream_t stream);
+
+/* covis_distance  (reference: src/droid.cpp:218-231, src/droid_kernels.cu:996-1090,2071-2091)
+ * dist[n] = fraction of frame i = ii[n]'s pixels that project outside the image under both
+ * Gj Gi^-1 with j = i-1 and j = i+1.  Entries with i < 1 or i+1 >= num_poses or
+ * i >= num_disps set HS2_DEV_BAD_INDEX in info[0] (the reference reads out of bounds).
+ */
+int hs2_covis_distance(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht,
+                       int wd, const float* intrinsics, const int64_t* ii, int64_t num, float* dist, int32_t* info,
+                       hs2_stream_t stream);
+
+/* depth_filter  (reference: src/droid.cpp:308-322, src/droid_kernels.cu:1094-1204,2093-2118)
+ * counter[b,i,j] (zeroed here) = number of neighbours k in {i-1,i-2,i-3,i+3,i+4,i+5} of frame
+ * i = ix[b] (inside the buffer) in which pixel (i,j)'s reprojected inverse depth lies within
+ * thresh[b] of one of the four disparities around the reprojection.  Needs num_poses >=
+ * num_disps; ix outside [0, num_disps) sets HS2_DEV_BAD_INDEX.
+ */
+int hs2_depth_filter(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht, int wd,
+                     const float* intrinsics, const int64_t* ix, const float* thresh, int64_t num, float* counter,
+                     int32_t* info, hs2_stream_t stream);
+
 /* Selects the kernels of the linearisation and Schur Gram for later hs2_ba calls
  * (process-wide; no counterpart in the reference, whose Gram is SIMT FP32 in
  * EEt6x6_kernel):

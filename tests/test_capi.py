@@ -93,6 +93,14 @@ def test_ops_check_contiguity_then_device():
 
 
 def test_out_of_path_ops_raise():
-    for name in ("pgba", "proj_trans", "covis_distance", "depth_filter", "iproj", "bi_inter"):
+    for name in ("pgba", "proj_trans", "bi_inter"):
         with pytest.raises(NotImplementedError, match=name):
             getattr(droid_backends, name)()
+
+
+def test_geometry_ops_check_inputs_on_cpu():
+    p, d = torch.zeros(4, 7), torch.ones(4, 3, 3)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        droid_backends.iproj(p, d, torch.zeros(4))
+    with pytest.raises(RuntimeError, match="contiguous"):
+        droid_backends.covis_distance(p, d.transpose(1, 2), torch.zeros(4), torch.ones(1, dtype=torch.long))
