@@ -44,6 +44,8 @@ SIGNATURES = {
                               _i32, _p, _p, _p, _p, _sz, _p],
     "hs2_ba_set_schur_path": [_i32],
     "hs2_iproj": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p],
+    "hs2_proj_trans": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _p, _i64, _i64, _p, _p, _p, _p],
+    "hs2_bi_inter": [_p, _i64, _i32, _i32, _p, _i32, _i32, _p, _p, _p, _p],
     "hs2_covis_distance": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _p],
     "hs2_depth_filter": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _i64, _p, _p, _p],
     "hs2_profile_enable": [_i32],

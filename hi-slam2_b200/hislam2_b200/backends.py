@@ -276,6 +276,59 @@ def depth_filter(poses, disps, intrinsics, ix, thresh):
     return counter
 
 
+def proj_trans(poses, disps, intrinsics, targets, weights, ii, jj):
+    """``droid_backends.proj_trans`` (reference ``src/droid.cpp:121-139``) -> [C, w], each
+    [M, H*W] for the M = len(unique(ii)) source frames in ascending order: the depth-only
+    Schur terms of the mono-prior alignment (``hislam2/geom/ba.py:178``)."""
+    dev = _geo_inputs("proj_trans", poses, disps, intrinsics,
+                      (("targets", targets), ("weights", weights), ("ii", ii), ("jj", jj)))
+    for name, t in (("targets", targets), ("weights", weights)):
+        _dtype(name, t, torch.float32)
+    _dtype("ii", ii, torch.int64)
+    _dtype("jj", jj, torch.int64)
+    E = ii.numel()
+    N, H, W = disps.shape
+    if jj.numel() != E or targets.shape != (E, 2, H, W) or weights.shape != (E, 2, H, W):
+        raise RuntimeError("proj_trans: targets/weights must be [E,2,H,W] and jj as long as ii")
+    if intrinsics.numel() < 4:
+        raise RuntimeError("proj_trans: intrinsics needs 4 values")
+    kx, slot = torch.unique(ii, sorted=True, return_inverse=True)
+    M = kx.numel()
+    C = torch.empty((M, H * W), dtype=torch.float32, device=dev)
+    w = torch.empty((M, H * W), dtype=torch.float32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    slot = slot.contiguous()
+    _lib.check(_lib.load().hs2_proj_trans(_ptr(poses), poses.shape[0], _ptr(disps), N, H, W, _ptr(intrinsics),
+                                          _ptr(targets), _ptr(weights), _ptr(ii), _ptr(jj), _ptr(slot), E, M,
+                                          _ptr(C), _ptr(w), _ptr(info), _stream(dev)), "proj_trans")
+    if E and int(info.item()) & _lib.HS2_DEV_BAD_INDEX:
+        raise RuntimeError("proj_trans: an edge index is outside the pose/disparity buffers")
+    return [C, w]
+
+
+def bi_inter(scales, grids):
+    """``droid_backends.bi_inter`` (reference ``src/droid.cpp:244-251``) -> [outputs [N,H,W],
+    jacobians [N,H,W,hs,ws]]: bilinear interpolation of each frame's scale grid at grids[b,i,j]
+    = (x, y) and its dense Jacobian (``hislam2/geom/ba.py:161-167``)."""
+    for name, t in (("scales", scales), ("grids", grids)):
+        _contig(name, t)
+        _cuda(name, t, scales.device)
+        _dtype(name, t, torch.float32)
+    if scales.dim() != 3 or grids.dim() != 4 or grids.shape[-1] != 2 or grids.shape[0] > scales.shape[0]:
+        raise RuntimeError("bi_inter: scales must be [N,hs,ws] and grids [N,H,W,2]")
+    dev = scales.device
+    N, H, W, _ = grids.shape
+    hs, ws = scales.shape[1:]
+    out = torch.zeros((N, H, W), dtype=torch.float32, device=dev)
+    jac = torch.empty((N, H, W, hs, ws), dtype=torch.float32, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_bi_inter(_ptr(scales), N, hs, ws, _ptr(grids), H, W, _ptr(out), _ptr(jac),
+                                        _ptr(info), _stream(dev)), "bi_inter")
+    if N and int(info.item()) & _lib.HS2_DEV_BAD_INDEX:
+        raise RuntimeError("bi_inter: a grid point's interpolation cell leaves the scale grid")
+    return [out, jac]
+
+
 # ------------------------------------------------------------------ corr_index
 def _corr_dtype(name, t):
     if t.dtype not in _DTYPES:

@@ -1,7 +1,10 @@
 // iproj / covis_distance / depth_filter: the per-pixel back-projection helpers of the
 // keyframe policy and of the point-cloud filter (reference: src/droid_kernels.cu
 // covis_distance_kernel :996-1090, depth_filter_kernel :1094-1204, iproj_kernel
-// :1208-1272, host wrappers :2071-2143).
+// :1208-1272, host wrappers :2071-2143); proj_trans / bi_inter: the two operators of the
+// mono-depth-prior alignment (JDSA, hislam2/geom/ba.py:161-219; reference
+// projective_transform2_kernel :246-362 + proj_trans_cuda :1781-1818, bi_inter_kernel
+// :1275-1316 + bi_inter_cuda :2145-2175).
 //
 // All three are one pass over disparity planes; the pose algebra matches the reference's
 // actSO3/relSE3 operation order (quat_rotate, relative_pose).
@@ -14,8 +17,17 @@
 //                   disparities around the reprojection (compared in double precision,
 //                   as the reference's 1.0/dj does).  Counts are small integers, so the
 //                   atomic sum is order-independent.
+//   proj_trans      CTA per edge: the depth-only Schur terms C = wu Jzu^2 + wv Jzv^2 and
+//                   w = wu ru Jzu + wv rv Jzv of every pixel (the ba linearisation without
+//                   the pose blocks), added with atomics into the row slot[e] of the edge's
+//                   source frame (the reference's accum_cuda over kx = unique(ii)).
+//   bi_inter        thread per pixel: bilinear interpolation of the frame's scale grid at
+//                   (x, y) and the four non-zero entries of the dense Jacobian
+//                   [N,H,W,hs,ws] (zeroed first), as the reference writes them.
 // Entries whose frame index lies outside the buffers (the reference reads out of bounds
 // there) set HS2_DEV_BAD_INDEX and produce no output for that entry.
+#include <algorithm>
+
 #include "common.cuh"
 #include "profile.cuh"
 
@@ -132,6 +144,76 @@ depth_filter_kernel(const float* __restrict__ poses, const float* __restrict__ d
   }
 }
 
+__global__ void __launch_bounds__(kGeoThreads)
+proj_trans_kernel(const float* __restrict__ poses, int64_t num_poses, const float* __restrict__ disps,
+                  int64_t num_disps, int ht, int wd, const float* __restrict__ intr,
+                  const float* __restrict__ targets, const float* __restrict__ weights,
+                  const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, const int64_t* __restrict__ slot,
+                  int64_t num_slots, float* __restrict__ C, float* __restrict__ w, int32_t* __restrict__ info) {
+  const int e = blockIdx.x;
+  const int64_t ix = ii[e], jx = jj[e], m = slot[e];
+  if (ix < 0 || jx < 0 || ix >= num_poses || jx >= num_poses || ix >= num_disps || m < 0 || m >= num_slots) {
+    if (threadIdx.x == 0) atomicOr(info, HS2_DEV_BAD_INDEX);
+    return;
+  }
+  const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
+  float tij[3], qij[4];
+  relative_pose(poses + 7 * ix, poses + 7 * ix + 3, poses + 7 * jx, poses + 7 * jx + 3, tij, qij);
+  const int HW = ht * wd;
+  const float* drow = disps + ix * HW;
+  const float* trg = targets + (int64_t)e * 2 * HW;
+  const float* wgt = weights + (int64_t)e * 2 * HW;
+  float* Cm = C + m * HW;
+  float* wm = w + m * HW;
+  for (int k = blockIdx.y * kGeoThreads + threadIdx.x; k < HW; k += gridDim.y * kGeoThreads) {
+    const int vi = k / wd;
+    const float u = (float)(k - vi * wd), v = (float)vi;
+    const float X[3] = {(u - cx) / fx, (v - cy) / fy, 1.0f};
+    const float h = drow[k];
+    float Y[3];
+    quat_rotate(qij, X, Y);
+    Y[0] += h * tij[0]; Y[1] += h * tij[1]; Y[2] += h * tij[2];
+    const bool bad = Y[2] < kMinDepth;
+    const float xp = fx * (Y[0] / Y[2]) + cx, yp = fy * (Y[1] / Y[2]) + cy;
+    const float d = bad ? 0.f : 1.0f / Y[2];
+    const float d2 = d * d;
+    const float wu = bad ? 0.f : 0.001f * wgt[k];
+    const float wv = bad ? 0.f : 0.001f * wgt[HW + k];
+    const float ru = trg[k] - xp, rv = trg[HW + k] - yp;
+    const float Jzu = fx * d * tij[0] + fx * (-Y[0] * d2) * tij[2];
+    const float Jzv = fy * d * tij[1] + fy * (-Y[1] * d2) * tij[2];
+    atomicAdd(&Cm[k], wu * Jzu * Jzu + wv * Jzv * Jzv);
+    atomicAdd(&wm[k], wu * ru * Jzu + wv * rv * Jzv);
+  }
+}
+
+__global__ void __launch_bounds__(kGeoThreads)
+bi_inter_kernel(const float* __restrict__ scales, int hs, int ws, const float* __restrict__ grids, int ht, int wd,
+                float* __restrict__ out, float* __restrict__ jac, int32_t* __restrict__ info) {
+  const int b = blockIdx.y;
+  const int HW = ht * wd;
+  const int k = blockIdx.x * kGeoThreads + threadIdx.x;
+  if (k >= HW) return;
+  const float x = grids[((int64_t)b * HW + k) * 2 + 0];
+  const float y = grids[((int64_t)b * HW + k) * 2 + 1];
+  const int x0 = (int)floorf(x), y0 = (int)floorf(y);
+  const int x1 = x0 + 1, y1 = y0 + 1;
+  if (!(x0 >= 0 && y0 >= 0 && x1 < ws && y1 < hs)) {   // also false for NaN
+    out[(int64_t)b * HW + k] = 0.f;
+    atomicOr(info, HS2_DEV_BAD_INDEX);
+    return;
+  }
+  const float wa = ((float)x1 - x) * ((float)y1 - y), wb = ((float)x1 - x) * (y - (float)y0);
+  const float wc = (x - (float)x0) * ((float)y1 - y), wdd = (x - (float)x0) * (y - (float)y0);
+  const float* S = scales + (int64_t)b * hs * ws;
+  out[(int64_t)b * HW + k] = wa * S[y0 * ws + x0] + wb * S[y1 * ws + x0] + wc * S[y0 * ws + x1] + wdd * S[y1 * ws + x1];
+  float* J = jac + ((int64_t)b * HW + k) * hs * ws;
+  J[y0 * ws + x0] = wa;
+  J[y1 * ws + x0] = wb;
+  J[y0 * ws + x1] = wc;
+  J[y1 * ws + x1] = wdd;
+}
+
 static int check_geo(const char* op, int64_t num_poses, int64_t num_disps, int ht, int wd) {
   if (num_poses < 0 || num_disps < 0 || ht <= 0 || wd <= 0 || (int64_t)ht * wd > (1 << 30)) {
     set_error("%s: bad sizes num_poses=%lld num_disps=%lld ht=%d wd=%d", op, (long long)num_poses,
@@ -216,5 +298,51 @@ extern "C" int hs2_depth_filter(const float* poses, int64_t num_poses, const flo
   depth_filter_kernel<<<dim3((unsigned)num, 6, (HW + kGeoThreads - 1) / kGeoThreads), kGeoThreads, 0, s>>>(
       poses, disps, num_disps, ht, wd, intrinsics, ix, thresh, counter, info);
   HS2_LAUNCH_CHECK("depth_filter_kernel");
+  return HS2_OK;
+}
+
+extern "C" int hs2_proj_trans(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht,
+                              int wd, const float* intrinsics, const float* targets, const float* weights,
+                              const int64_t* ii, const int64_t* jj, const int64_t* slot, int64_t num_edges,
+                              int64_t num_slots, float* C, float* w, int32_t* info, hs2_stream_t stream) {
+  using namespace hs2;
+  int rc = check_geo("proj_trans", num_poses, num_disps, ht, wd);
+  if (rc) return rc;
+  if (num_edges < 0 || num_edges > 0x7fffffff || num_slots < 0) {
+    set_error("proj_trans: bad counts (edges %lld, slots %lld)", (long long)num_edges, (long long)num_slots);
+    return HS2_ERR_INVALID;
+  }
+  if (num_slots == 0) return HS2_OK;
+  if ((rc = bind_device(C))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int HW = ht * wd;
+  HS2_CUDA(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)num_slots * HW, s));
+  HS2_CUDA(cudaMemsetAsync(w, 0, sizeof(float) * (size_t)num_slots * HW, s));
+  if (num_edges == 0) return HS2_OK;
+  const int ysplit = std::min(8, (HW + kGeoThreads - 1) / kGeoThreads);
+  HS2_PROF("proj_trans", s);
+  proj_trans_kernel<<<dim3((unsigned)num_edges, ysplit), kGeoThreads, 0, s>>>(
+      poses, num_poses, disps, num_disps, ht, wd, intrinsics, targets, weights, ii, jj, slot, num_slots, C, w, info);
+  HS2_LAUNCH_CHECK("proj_trans_kernel");
+  return HS2_OK;
+}
+
+extern "C" int hs2_bi_inter(const float* scales, int64_t num, int hs, int ws, const float* grids, int ht, int wd,
+                            float* outputs, float* jacobians, int32_t* info, hs2_stream_t stream) {
+  using namespace hs2;
+  if (num < 0 || num > 65535 || hs <= 0 || ws <= 0 || ht <= 0 || wd <= 0 || (int64_t)ht * wd > (1 << 30)) {
+    set_error("bi_inter: bad sizes num=%lld hs=%d ws=%d ht=%d wd=%d", (long long)num, hs, ws, ht, wd);
+    return HS2_ERR_INVALID;
+  }
+  if (num == 0) return HS2_OK;
+  int rc = bind_device(outputs);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int HW = ht * wd;
+  HS2_CUDA(cudaMemsetAsync(jacobians, 0, sizeof(float) * (size_t)num * HW * hs * ws, s));
+  HS2_PROF("bi_inter", s);
+  bi_inter_kernel<<<dim3((HW + kGeoThreads - 1) / kGeoThreads, (unsigned)num), kGeoThreads, 0, s>>>(
+      scales, hs, ws, grids, ht, wd, outputs, jacobians, info);
+  HS2_LAUNCH_CHECK("bi_inter_kernel");
   return HS2_OK;
 }

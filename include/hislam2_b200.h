@@ -200,6 +200,27 @@ int hs2_depth_filter(const float* poses, int64_t num_poses, const float* disps, 
                      const float* intrinsics, const int64_t* ix, const float* thresh, int64_t num, float* counter,
                      int32_t* info, hs2_stream_t stream);
 
+/* proj_trans  (reference: src/droid.cpp:121-139, src/droid_kernels.cu:246-362,1781-1818)
+ * Depth-only Schur terms of the mono-prior alignment: per edge e and pixel,
+ * C = wu Jzu^2 + wv Jzv^2 and w = wu ru Jzu + wv rv Jzv (the ba linearisation without the
+ * pose blocks), summed into row slot[e] of C, w [num_slots, H*W] (zeroed here).  The
+ * reference sums over kx = unique(ii) (accum_cuda); slot[e] is the position of ii[e] in kx.
+ * intrinsics: the 4 values of the camera (the reference reads row 0 of an [N,4] tensor).
+ */
+int hs2_proj_trans(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht, int wd,
+                   const float* intrinsics, const float* targets, const float* weights, const int64_t* ii,
+                   const int64_t* jj, const int64_t* slot, int64_t num_edges, int64_t num_slots, float* C, float* w,
+                   int32_t* info, hs2_stream_t stream);
+
+/* bi_inter  (reference: src/droid.cpp:244-251, src/droid_kernels.cu:1275-1316,2145-2175)
+ * outputs[b,i,j] = bilinear interpolation of scales[b] ([hs, ws]) at grids[b,i,j] = (x, y),
+ * jacobians[b,i,j] ([hs, ws], zeroed here) = its four interpolation weights.  Grid points
+ * whose 2x2 cell leaves the scale grid set HS2_DEV_BAD_INDEX (the reference writes out of
+ * bounds there).
+ */
+int hs2_bi_inter(const float* scales, int64_t num, int hs, int ws, const float* grids, int ht, int wd,
+                 float* outputs, float* jacobians, int32_t* info, hs2_stream_t stream);
+
 /* Selects the kernels of the linearisation and Schur Gram for later hs2_ba calls
  * (process-wide; no counterpart in the reference, whose Gram is SIMT FP32 in
  * EEt6x6_kernel):

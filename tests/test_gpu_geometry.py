@@ -67,3 +67,33 @@ def test_depth_filter_rejects_bad_index(cuda):
     with pytest.raises(RuntimeError, match="ix outside"):
         droid_backends.depth_filter(poses, disps, intr, torch.tensor([12], device=cuda),
                                     torch.ones(1, device=cuda))
+
+
+def test_proj_trans_matches_oracle(cuda):
+    p = synth.make_ba_problem("frontend", seed=3)
+    q = {k: (v.to(cuda) if torch.is_tensor(v) else v) for k, v in p.items()}
+    intr2 = q["intrinsics"][None].contiguous()
+    C, w = droid_backends.proj_trans(q["poses"], q["disps"], intr2, q["targets"], q["weights"], q["ii"], q["jj"])
+    Co, wo = oracle.geometry.proj_trans(p["poses"].numpy(), p["disps"].numpy(), p["intrinsics"].numpy(),
+                                        p["targets"].numpy(), p["weights"].numpy(), p["ii"].numpy(), p["jj"].numpy())
+    assert C.shape == Co.shape
+    for got, ref in ((C, Co), (w, wo)):
+        got = got.double().cpu().numpy()
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 1e-5, err
+
+
+def test_bi_inter_matches_oracle(cuda):
+    g = torch.Generator().manual_seed(5)
+    M, ht, wd, hs, ws = 3, 43, 77, 6, 8
+    scales = (0.5 + torch.rand(M, hs, ws, generator=g)).to(cuda)
+    mx, my = torch.meshgrid(torch.linspace(0, hs - 1 - 1e-6, ht), torch.linspace(0, ws - 1 - 1e-6, wd), indexing="ij")
+    grids = torch.stack((my, mx), -1)[None].expand(M, -1, -1, -1).contiguous().to(cuda)
+    out, jac = droid_backends.bi_inter(scales, grids)
+    ro, rj = oracle.geometry.bi_inter(scales.cpu().numpy(), grids.cpu().numpy())
+    np.testing.assert_allclose(out.cpu().numpy(), ro, rtol=2e-6, atol=2e-6)
+    np.testing.assert_allclose(jac.cpu().numpy(), rj, rtol=2e-6, atol=2e-6)
+    bad = grids.clone()
+    bad[0, 0, 0, 0] = ws - 1.0                     # cell would leave the grid
+    with pytest.raises(RuntimeError, match="leaves the scale grid"):
+        droid_backends.bi_inter(scales, bad)

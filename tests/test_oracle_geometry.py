@@ -93,3 +93,49 @@ def test_depth_filter_matches_loop():
                         cnt += any(abs(1.0 / dj - 1.0 / dd) < thresh[b] for dd in ds)
                 assert got[b, y, x] == cnt
     assert got.max() >= 2
+
+
+def test_proj_trans_matches_loop():
+    poses, disps, intr = _case(3, K=5, ht=4, wd=5)
+    rng = np.random.default_rng(3)
+    ii = np.array([0, 0, 2, 3, 3, 1])
+    jj = np.array([1, 2, 3, 2, 4, 1])            # includes a self edge (1 -> 1)
+    E, (ht, wd) = len(ii), disps.shape[1:]
+    targets = rng.uniform(0, 5, size=(E, 2, ht, wd))
+    weights = rng.uniform(0, 2, size=(E, 2, ht, wd))
+    C, w = oracle.geometry.proj_trans(poses, disps, intr[None], targets, weights, ii, jj)
+    kx = np.unique(ii)
+    assert C.shape == (len(kx), ht * wd)
+    fx, fy, cx, cy = intr
+    Cl, wl = np.zeros_like(C), np.zeros_like(w)
+    for e in range(E):
+        m = int(np.searchsorted(kx, ii[e]))
+        t, q = _rel(poses[ii[e]], poses[jj[e]])
+        for y in range(ht):
+            for x in range(wd):
+                h = disps[ii[e], y, x]
+                Y = _rot(q, np.array([(x - cx) / fx, (y - cy) / fy, 1.0])) + h * t
+                if Y[2] < 0.25:
+                    continue
+                d = 1.0 / Y[2]
+                ju = fx * d * t[0] - fx * Y[0] * d * d * t[2]
+                jv = fy * d * t[1] - fy * Y[1] * d * d * t[2]
+                wu, wv = 0.001 * weights[e, 0, y, x], 0.001 * weights[e, 1, y, x]
+                ru = targets[e, 0, y, x] - (fx * Y[0] / Y[2] + cx)
+                rv = targets[e, 1, y, x] - (fy * Y[1] / Y[2] + cy)
+                Cl[m, y * wd + x] += wu * ju * ju + wv * jv * jv
+                wl[m, y * wd + x] += wu * ru * ju + wv * rv * jv
+    np.testing.assert_allclose(C, Cl, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(w, wl, rtol=1e-12, atol=1e-15)
+
+
+def test_bi_inter_properties():
+    rng = np.random.default_rng(4)
+    scales = rng.uniform(0.5, 2.0, size=(2, 3, 4))
+    grids = np.stack([rng.uniform(0, 3 - 1e-6, size=(2, 5, 6)), rng.uniform(0, 2 - 1e-6, size=(2, 5, 6))], -1)
+    grids[0, 0, 0] = (2.0, 1.0)                   # a grid node: exact value
+    out, jac = oracle.geometry.bi_inter(scales, grids)
+    np.testing.assert_allclose(jac.sum(axis=(-1, -2)), 1.0, rtol=1e-12)
+    np.testing.assert_allclose(out, np.einsum("bijyx,byx->bij", jac, scales), rtol=1e-12)
+    assert abs(out[0, 0, 0] - scales[0, 1, 2]) < 1e-12
+    assert ((jac > 0).sum(axis=(-1, -2)) <= 4).all()
