@@ -1521,6 +1521,13 @@ __device__ __forceinline__ bool wait_flag(const unsigned* f, int32_t* info) {
   return true;
 }
 
+// d(8x8, two values per lane) += a(8x4) b(4x8) in FP64 on the tensor cores (mma.sync
+// m8n8k4): lane l holds a[l/4][l%4], b[l%4][l/4] and d[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
 // (b) One warp factors the nsb x nsb diagonal sub-block at (c0, c0) in registers,
 // fraction-free: step j replaces the trailing entries by (A_rk d_j - A_rj A_kj) 2^-E_j,
 // d_j the pivot and E_j its binary exponent, so no reciprocal sits on the dependency
@@ -1627,35 +1634,35 @@ __device__ bool chol_panel(int n, int kb, int t, double* __restrict__ A, double*
   for (int c0 = 0; c0 < nb; c0 += 16) {
     const int c1 = min(c0 + 16, nb);
     if (c0 > 0) {
-      // (a) left-looking update of the sub-panel columns c0 + 2q + h of row r
-      const int r = tid >> 1, h = tid & 1;
-      const bool xrow = r >= kNB;
-      if (xrow ? (r - kNB < nr) : (r >= c0 && r < nb)) {
-        double acc[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+      const int lane = tid & 31, warp = tid >> 5;
+      // (a) left-looking update of the sub-panel columns [c0, c0+16) of the rows >= c0 and the
+      // X rows by FP64 tensor-core MMA (m8n8k4): a warp owns an 8-row tile and both 8-column
+      // halves, k runs over the c0 columns already eliminated.
+      const int td = (((nb + 7) >> 3) - (c0 >> 3)), tx = (nr + 7) >> 3;
+      for (int tile = warp; tile < td + tx; tile += kCholThreads / 32) {
+        const int rt = tile < td ? c0 + 8 * tile : kNB + 8 * (tile - td);
+        double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+        for (int k0 = 0; k0 < c0; k0 += 4) {
+          const double av = Pm[rt + (lane >> 2)][k0 + (lane & 3)];
+          const double b0 = Pm[c0 + (lane >> 2)][k0 + (lane & 3)];
+          const double b1 = Pm[c0 + 8 + (lane >> 2)][k0 + (lane & 3)];
+          dmma_m8n8k4(d00, d01, av, b0);
+          dmma_m8n8k4(d10, d11, av, b1);
+        }
+        double* row = Pm[rt + (lane >> 2)] + c0 + (lane & 3) * 2;
+        row[0] -= d00;
+        row[1] -= d01;
+        row[8] -= d10;
+        row[9] -= d11;
+      }
+      if (tid < c1 - c0) {
+        const int r = c0 + tid;
+        double b0 = 0.0, b1 = 0.0;
         for (int k = 0; k < c0; k += 2) {
-          const double2 pr = *reinterpret_cast<const double2*>(&Pm[r][k]);
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const double2 pl = *reinterpret_cast<const double2*>(&Pm[c0 + 2 * q + h][k]);
-            acc[q] = fma(pr.x, pl.x, acc[q]);
-            acc[q] = fma(pr.y, pl.y, acc[q]);
-          }
+          b0 = fma(Pm[r][k], bv[k], b0);
+          b1 = fma(Pm[r][k + 1], bv[k + 1], b1);
         }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int l = c0 + 2 * q + h;
-          if (l < c1) Pm[r][l] -= acc[q];
-        }
-        if (h == 0 && !xrow && r < c1) {
-          double b0 = 0.0, b1 = 0.0;
-          for (int k = 0; k < c0; k += 2) {
-            b0 = fma(Pm[r][k], bv[k], b0);
-            b1 = fma(Pm[r][k + 1], bv[k + 1], b1);
-          }
-          bv[r] -= b0 + b1;
-        }
+        bv[r] -= b0 + b1;
       }
       __syncthreads();
     }
