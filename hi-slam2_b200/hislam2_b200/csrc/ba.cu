@@ -778,6 +778,7 @@ constexpr int kTcThreads = 320;
 constexpr int kTcSplitWarps = 8;
 constexpr int kTcK = 32;                       // pixels per stage (128 B per plane row)
 constexpr int kTcMaxStages = 6;                // stages of frames of <= 128 tile rows
+constexpr int kTcSkip = 112;                   // Gram columns M tile 1 leaves out (< 6 * 21, 8-row aligned)
 constexpr int kTcMaxBlocks = 42;               // N <= 6*42 + 1 <= 256
 constexpr int kTcRows = 256;                   // plane rows per tile
 constexpr int kTcBox = 64;                     // plane rows per TMA box
@@ -963,7 +964,9 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     }
   } else if (lane == 0) {
     // ------------------------------------------------------------- MMA issuer
-    const uint32_t idesc = umma_idesc_tf32(128, Npad);
+    // M tile 1 (rows >= 128) only needs the columns of blocks b >= a >= 21, i.e. from 126 on:
+    // its B operand starts at row kTcSkip (a multiple of 8 rows, N stays a multiple of 16)
+    const uint32_t idesc0 = umma_idesc_tf32(128, Npad), idesc1 = umma_idesc_tf32(128, Npad - kTcSkip);
     for (int c = 0; c < nchunks; ++c) {
       const int st = c % nst;
       if (!mbar_wait(bar_full + 8 * st, (c / nst) & 1, abort_flag)) break;
@@ -973,13 +976,15 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
       for (int mt = 0; mt < mtiles; ++mt) {
         const uint32_t a_hi = b_hi + mt * 128 * 128;
         const uint32_t a_lo = b_lo + mt * 128 * 128;
+        const uint32_t boff = mt ? kTcSkip * 128u : 0u;
+        const uint32_t idesc = mt ? idesc1 : idesc0;
         const uint32_t d = tmem + (uint32_t)(mt * Npad);
 #pragma unroll
         for (int k = 0; k < kTcK / 8; ++k) {
           const uint32_t kb = k * 32;
-          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + kb), idesc, (c | k) ? 1u : 0u);
-          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + kb), idesc, 1u);
-          umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + kb), idesc, 1u);
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + boff + kb), idesc, (c | k) ? 1u : 0u);
+          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + boff + kb), idesc, 1u);
+          umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + boff + kb), idesc, 1u);
         }
       }
       umma_commit(bar_empty + 8 * st);
@@ -998,7 +1003,8 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
       const bool mrow = ok && R < 6 * nr;
       const int a = R / 6, x = R % 6;
       const int pa = mrow ? spose[a] : 0;
-      for (int col0 = (warp >> 2) * 16; col0 < Npad; col0 += 32) {
+      const int cbase = mt ? kTcSkip : 0;             // first Gram column held by this M tile
+      for (int col0 = (warp >> 2) * 16; cbase + col0 < Npad; col0 += 32) {
         uint32_t v[16];
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * Npad + col0);
         asm volatile(
@@ -1010,7 +1016,7 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
         if (!mrow) continue;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int col = col0 + j;
+          const int col = cbase + col0 + j;
           const double val = -(double)__uint_as_float(v[j]);
           if (col < 6 * nr) {
             const int b = col / 6, y = col % 6;

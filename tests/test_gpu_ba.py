@@ -70,11 +70,12 @@ def oracle_reduced_system(p, motion_only=False):
     return it["A"] - it["S"], it["b"] - it["bS"]
 
 
-def star_problem():
-    """60 frames of the 300-kf workload plus 48 edges out of frame 12: its depth frame has
-    49 Schur rows, past the tensor-core Gram's limit of 42, so both Gram kernels run."""
+def star_problem(extra=48):
+    """60 frames of the 300-kf workload plus `extra` edges out of frame 12.  With 48 its depth
+    frame has 49 Schur rows, past the tensor-core Gram's limit of 42, so both Gram kernels run;
+    with 24 it has about 30 (two 128-row M tiles of the tensor-core Gram)."""
     p = subproblem(synth.make_ba_problem("backend300", seed=3), 60)
-    extra_j = torch.arange(13, 61) % 60
+    extra_j = torch.arange(13, 13 + extra) % 60
     extra_j[extra_j == 12] = 0
     extra_i = torch.full_like(extra_j, 12)
     coords = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], extra_i, extra_j)
@@ -82,7 +83,7 @@ def star_problem():
     q["ii"] = torch.cat([p["ii"], extra_i])
     q["jj"] = torch.cat([p["jj"], extra_j])
     q["targets"] = torch.cat([p["targets"], coords.permute(0, 3, 1, 2).float()]).contiguous()
-    q["weights"] = torch.cat([p["weights"], torch.full_like(p["weights"][:48], 0.5)]).contiguous()
+    q["weights"] = torch.cat([p["weights"], torch.full_like(p["weights"][:extra], 0.5)]).contiguous()
     return q
 
 
@@ -91,6 +92,7 @@ CASES = {
     "frontend": lambda: synth.make_ba_problem("frontend", seed=1),
     "backend40": lambda: subproblem(synth.make_ba_problem("backend300", seed=2), 40),
     "star60": star_problem,
+    "wide60": lambda: star_problem(extra=24),
 }
 
 
