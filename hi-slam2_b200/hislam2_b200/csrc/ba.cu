@@ -88,7 +88,7 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
   L.L11 = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB * kNB);
   L.dinv = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB);
   L.ychol = take(sizeof(double) * (size_t)(n + 1));
-  L.ctl = take(sizeof(unsigned) * (4 + (size_t)((n + kNB - 1) / kNB)));   // barrier words + ready flags
+  L.ctl = take(sizeof(unsigned) * (4 + 2 * (size_t)((n + kNB - 1) / kNB)));   // barrier words, ready flags, slice counters
   L.total = o;
   return L;
 }
@@ -1434,9 +1434,10 @@ static int encode_erows_map(CUtensorMap* map, float* erows, int HW, int64_t plan
 //   damping   diag += ep + lm*diag                                          | barrier
 //   panel 0                                                                 | barrier
 //   for kb = 0 .. nbk-2 (look-ahead by one panel)
-//     A   column block kb+1 -= L[:, kb] L[kb+1, kb]^T in 16-row slices      | barrier
-//     B   panel kb+1 on `rest` CTAs, in parallel with the remaining tiles
-//         of update kb (column blocks kb+2 ..) on the other CTAs             | barrier
+//     A   column block kb+1 -= L[:, kb] L[kb+1, kb]^T in 16-row slices      | per-row counters
+//     B   panel kb+1 on `rest` CTAs (each waits for its two block rows'
+//         slices), in parallel with the remaining tiles of update kb
+//         (column blocks kb+2 ..) on the other CTAs                         | barrier
 //   backward  x_c = L_cc^-T (y_c - sum_{j>c} L_jc^T x_j), one CTA per block c,
 //             ordered by per-block ready flags instead of grid barriers
 //
@@ -1462,7 +1463,8 @@ struct CholBuf {
   double* L11;      // [nbk][64][64] factored diagonal blocks (zero above the diagonal)
   double* dinv;     // [nbk][64] reciprocals of their diagonals
   double* y;        // [n] forward-substituted right-hand side
-  unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed, [4 + c] ready flags
+  unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed, [4 + c] ready flags,
+                    // [4 + nbk + R] phase-A slices done on block row R
 };
 
 __device__ __forceinline__ double2 ldcg2(const double* p) {
@@ -1512,6 +1514,35 @@ __device__ __forceinline__ bool grid_barrier(unsigned* ctl, unsigned nblocks, in
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+__device__ __forceinline__ void red_release_add_gpu(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Panel kb+1, task t reads block rows kb+1 (D) and kb+1+t (X) of column block kb+1: waits
+// until the four phase-A slices of each have been applied for every panel up to kb.
+__device__ bool chol_wait_slices(const unsigned* slices, int kb, int t, int32_t* info) {
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) {
+    const unsigned target = 4u * (unsigned)(kb + 1);
+    int bad = 0;
+    for (int k = 0; k < (t > 0 ? 2 : 1) && !bad; ++k) {
+      const unsigned* c = slices + kb + 1 + (k ? t : 0);
+      unsigned spins = 0;
+      while (ld_acquire_gpu(c) < target) {
+        if (++spins > kBarrierSpins) {
+          atomicOr(info, HS2_DEV_TIMEOUT);
+          bad = 1;
+          break;
+        }
+        if (spins > 64) __nanosleep(32);
+      }
+    }
+    s_bad = bad;
+  }
+  __syncthreads();
+  return s_bad == 0;
 }
 
 // Waits (thread 0) until the ready flag is set; false on timeout.
@@ -1912,12 +1943,16 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
   for (int kb = 0; kb + 1 < nbk && !failed; ++kb) {
     const int o = kb * kNB;
     const int rest = nbk - kb - 1;
-    // A: column block kb+1, 16-row slices of the tiles below panel kb
+    // A: column block kb+1, 16-row slices of the tiles below panel kb; each slice counts
+    // itself on its block row (release), which the panel tasks of phase B wait for instead
+    // of a grid barrier
+    unsigned* slices = cb.ctl + kCtlFlags + nbk;
     for (int t = blockIdx.x; t < rest * 4; t += G) {
       const int I = t >> 2, q = t & 3;
       chol_update_tile<1>(n, A, o, o + kNB + I * kNB + 16 * q, o + kNB, I == 0, csm);
+      __syncthreads();
+      if (threadIdx.x == 0) red_release_add_gpu(slices + kb + 1 + I, 1u);
     }
-    if (!grid_barrier(cb.ctl, G, info)) return;
     // B: panel kb+1 (tasks 0..rest-1) || tiles (I, J), 1 <= J <= I < rest, of update kb.
     // The panel tasks sit on CTAs of their own (they are the longer tasks); the tiles go
     // round-robin over the remaining CTAs.
@@ -1925,9 +1960,13 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
     const bool split = (int)G > rest;
     const int tfirst = split ? ((int)blockIdx.x < rest ? ntiles : (int)blockIdx.x - rest) : (int)blockIdx.x;
     const int tstep = split ? (int)G - rest : (int)G;
-    if (split && (int)blockIdx.x < rest) chol_panel(n, kb + 1, blockIdx.x, A, bvec, cb, csm);
+    if (split && (int)blockIdx.x < rest) {
+      if (!chol_wait_slices(slices, kb, blockIdx.x, info)) return;
+      chol_panel(n, kb + 1, blockIdx.x, A, bvec, cb, csm);
+    }
     for (int t = tfirst; t < (split ? ntiles : rest + ntiles); t += tstep) {
       if (!split && t < rest) {
+        if (!chol_wait_slices(slices, kb, t, info)) return;
         chol_panel(n, kb + 1, t, A, bvec, cb, csm);
         continue;
       }
@@ -2095,7 +2134,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   }
   const int work = std::max(std::max(nbk, (nbk - 1) * nbk / 2), (n + kCholThreads - 1) / kCholThreads);
   int G = std::max(1, std::min(grid_cap[dev], work));
-  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + nbk) * sizeof(unsigned), s));
+  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + 2 * nbk) * sizeof(unsigned), s));
   void* args[] = {&n, &lm, &ep, &w, &cb, &dx, &info};
   HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_cholesky_kernel, dim3(G), dim3(kCholThreads), args, smem, s));
   HS2_LAUNCH_CHECK("ba_cholesky_kernel");
