@@ -321,18 +321,21 @@ __global__ void ba_kk_kernel(const int64_t* __restrict__ ii, int E, int t0, int 
 }
 
 // ---------------------------------------------------------- edge setup ---
+// Six threads per edge: lane c of the group forms column c of L (the FP64 map Ji = L Jj);
+// lane 0 also writes Gij and its rotation matrix.
 __global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int64_t* __restrict__ ii,
                                      const int64_t* __restrict__ jj, int E, float* __restrict__ etab,
                                      double* __restrict__ etab64, const int32_t* __restrict__ info) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gid / 6, c = gid - (gid / 6) * 6;
   if (e >= E || info[0]) return;
   const int64_t a = ii[e], b = jj[e];
   float tij[3], qij[4];
   relative_pose(poses + 7 * a, poses + 7 * a + 3, poses + 7 * b, poses + 7 * b + 3, tij, qij);
   float* t = etab + (int64_t)e * kEtab;
-  t[0] = tij[0]; t[1] = tij[1]; t[2] = tij[2];
-  t[3] = qij[0]; t[4] = qij[1]; t[5] = qij[2]; t[6] = qij[3]; t[7] = 0.f;
-  {
+  if (c == 0) {
+    t[0] = tij[0]; t[1] = tij[1]; t[2] = tij[2];
+    t[3] = qij[0]; t[4] = qij[1]; t[5] = qij[2]; t[6] = qij[3]; t[7] = 0.f;
     // rotation matrix of qij (row-major) at 44..52
     const float x = qij[0], y = qij[1], z = qij[2], ww = qij[3];
     float* R = t + 44;
@@ -343,16 +346,14 @@ __global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int6
   }
   const double td[3] = {tij[0], tij[1], tij[2]};
   const double qd[4] = {qij[0], qij[1], qij[2], qij[3]};
+  double u[6] = {0, 0, 0, 0, 0, 0};
+  u[c] = 1.0;
+  double col[6];
+  pose_jacobian_i(td, qd, u, col);
   double* L64 = etab64 + (int64_t)e * 36;
-  for (int c = 0; c < 6; ++c) {
-    double u[6] = {0, 0, 0, 0, 0, 0};
-    u[c] = 1.0;
-    double col[6];
-    pose_jacobian_i(td, qd, u, col);
-    for (int r = 0; r < 6; ++r) {
-      L64[r * 6 + c] = col[r];
-      t[8 + r * 6 + c] = (float)col[r];
-    }
+  for (int r = 0; r < 6; ++r) {
+    L64[r * 6 + c] = col[r];
+    t[8 + r * 6 + c] = (float)col[r];
   }
 }
 
@@ -538,53 +539,71 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
 }
 
 // ------------------------------------------------------------- assemble ---
+// Six threads per edge: lane r of the group adds row r of Hjj / vj (block j), of
+// Hii = L Hjj L^T / vi = L vj (block i) and of Hij = L Hjj (lower block triangle).
 __global__ void ba_assemble_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, int E, int t0,
                                    int P, BaPtrs w, const int32_t* __restrict__ info) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gid / 6, r = gid - (gid / 6) * 6;
   if (e >= E || info[0]) return;
   const int i = (int)(ii[e] - t0), j = (int)(jj[e] - t0);
   if (i < 0 && j < 0) return;
   const double* h = w.hedge + (int64_t)e * 27;
   const double* L = w.etab64 + (int64_t)e * 36;
   double Hjj[6][6], vj[6];
-  for (int r = 0; r < 6; ++r) {
-    vj[r] = h[21 + r];
-    for (int c = r; c < 6; ++c) Hjj[r][c] = Hjj[c][r] = h[tri6(r, c)];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    vj[a] = h[21 + a];
+#pragma unroll
+    for (int c = a; c < 6; ++c) Hjj[a][c] = Hjj[c][a] = h[tri6(a, c)];
   }
   const int64_t n = 6 * (int64_t)P;
   double* A = w.A;
   if (j >= 0) {
-    for (int r = 0; r < 6; ++r) {
-      atomicAdd(&w.b[j * 6 + r], vj[r]);
-      for (int c = 0; c < 6; ++c) atomicAdd(&A[(j * 6 + r) * n + j * 6 + c], Hjj[r][c]);
-    }
+    atomicAdd(&w.b[j * 6 + r], vj[r]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) atomicAdd(&A[(j * 6 + r) * n + j * 6 + c], Hjj[r][c]);
   }
   if (i < 0) return;
-  double Hij[6][6];
-  for (int r = 0; r < 6; ++r)
-    for (int c = 0; c < 6; ++c) {
-      double acc = 0.0;
-      for (int k = 0; k < 6; ++k) acc += L[r * 6 + k] * Hjj[k][c];
-      Hij[r][c] = acc;
-    }
-  for (int r = 0; r < 6; ++r) {
-    double vi = 0.0;
-    for (int k = 0; k < 6; ++k) vi += L[r * 6 + k] * vj[k];
-    atomicAdd(&w.b[i * 6 + r], vi);
-    for (int c = 0; c < 6; ++c) {
-      double acc = 0.0;
-      for (int k = 0; k < 6; ++k) acc += Hij[r][k] * L[c * 6 + k];
-      atomicAdd(&A[(i * 6 + r) * n + i * 6 + c], acc);
-    }
+  double Lr[6], Hij[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) Lr[k] = L[r * 6 + k];
+  double vi = 0.0;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc += Lr[k] * Hjj[k][c];
+    Hij[c] = acc;
+    vi += Lr[c] * vj[c];
+  }
+  atomicAdd(&w.b[i * 6 + r], vi);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc += Hij[k] * L[c * 6 + k];
+    atomicAdd(&A[(i * 6 + r) * n + i * 6 + c], acc);
   }
   if (j < 0) return;
   // only the lower block triangle of the system is kept (the factorisation reads nothing else)
-  for (int r = 0; r < 6; ++r)
+  if (i > j) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) atomicAdd(&A[(i * 6 + r) * n + j * 6 + c], Hij[c]);
+  } else if (j > i) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) atomicAdd(&A[(j * 6 + c) * n + i * 6 + r], Hij[c]);
+  } else {
+    // i == j (self edge): Hij + Hij^T on the diagonal block; the transpose row needs the
+    // other lanes' Hij, formed here from L and Hjj directly
+#pragma unroll
     for (int c = 0; c < 6; ++c) {
-      if (i > j) atomicAdd(&A[(i * 6 + r) * n + j * 6 + c], Hij[r][c]);
-      else if (j > i) atomicAdd(&A[(j * 6 + c) * n + i * 6 + r], Hij[r][c]);
-      else atomicAdd(&A[(i * 6 + r) * n + i * 6 + c], Hij[r][c] + Hij[c][r]);
+      double tcr = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) tcr += L[c * 6 + k] * Hjj[k][r];
+      atomicAdd(&A[(i * 6 + r) * n + i * 6 + c], Hij[c] + tcr);
     }
+  }
 }
 
 // ---------------------------------------------------------------- schur ---
@@ -2191,7 +2210,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
   const int64_t S = std::min<int64_t>(p.K, (int64_t)P + E);
   if (E > 0) {
     HS2_PROF("ba_edge_setup", s);
-    ba_edge_setup_kernel<<<(E + 127) / 128, 128, 0, s>>>(poses, ii, jj, E, w.etab, w.etab64, info);
+    ba_edge_setup_kernel<<<(6 * E + 127) / 128, 128, 0, s>>>(poses, ii, jj, E, w.etab, w.etab64, info);
     HS2_LAUNCH_CHECK("ba_edge_setup_kernel");
     HS2_CUDA(cudaMemsetAsync(w.hedge, 0, sizeof(double) * 27 * (size_t)E, s));
   }
@@ -2226,7 +2245,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
   }
   if (E > 0 && n > 0) {
     HS2_PROF("ba_assemble", s);
-    ba_assemble_kernel<<<(E + 127) / 128, 128, 0, s>>>(ii, jj, E, p.t0, P, w, info);
+    ba_assemble_kernel<<<(6 * E + 127) / 128, 128, 0, s>>>(ii, jj, E, p.t0, P, w, info);
     HS2_LAUNCH_CHECK("ba_assemble_kernel");
   }
   if (!p.motion_only && n > 0 && S > 0) {
