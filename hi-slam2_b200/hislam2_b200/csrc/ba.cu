@@ -1585,17 +1585,21 @@ __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, do
 }
 
 // (b) One warp factors the nsb x nsb diagonal sub-block at (c0, c0) in registers,
-// fraction-free: step j replaces the trailing entries by (A_rk d_j - A_rj A_kj) 2^-E_j,
-// d_j the pivot and E_j its binary exponent, so no reciprocal sits on the dependency
-// chain from one pivot to the next (the power-of-two scale is exact and keeps the
-// entries in range).  After step j the trailing block equals c_{j+1} times the true
-// Schur complement, c_{j+1} = c_j d_j 2^-E_j, so with s_j = 1/sqrt(c_j d_j):
-//   L_rj = A_rj s_j,   1/L_jj = c_j s_j,   y_j = b_j s_j.
-// Lane = row (0..15) + 16 * column half; a lane holds the 8 entries of its row in its
-// half, padded with the identity outside nsb.  Column j (and b_j) is exchanged
-// through a double-buffered 2 x 20 shared array, one __syncwarp per step.  Writes L
-// (lower part), the multipliers M_rj = L_rj / L_jj above the diagonal (row j), 1/L_jj
-// to sv and y to bv.
+// fraction-free with 2 x 2 pivot blocks: with u, v the trailing columns j, j+1, the block
+// P = [p q; q s] and det = p s - q^2, step (j, j+1) replaces the trailing entries by
+//   (A_rk det - [u_r v_r] adj(P) [u_k v_k]^T) 2^-E,   E the binary exponent of det,
+// so no reciprocal sits on the chain from one pivot block to the next and the exact
+// power-of-two scale keeps the entries in range.  The trailing block is then c times the
+// true Schur complement, c <- c det 2^-E.  Eliminating column j alone would give the
+// scale c p and column j+1 the entries w_r = p v_r - q u_r with pivot det, so with
+// cd = (c p, c p det) and f = (c, c p) for the two columns:
+//   L_rk = num_rk / sqrt(cd_k),   1/L_kk = f_k / sqrt(cd_k),   y_k = b'_k / sqrt(cd_k),
+// num = u_r resp. w_r and b' = b_j resp. p b_j+1 - q b_j.  The products are recorded per
+// column and L is formed after the loop, off the elimination chain.  Lane = row (0..15)
+// + 16 * column half; a lane holds the 8 entries of its row in its half, padded with the
+// identity outside nsb.  Columns j, j+1 (and b_j, b_j+1) are exchanged through a double-
+// buffered 2 x 36 shared array, one __syncwarp per block step.  Writes L (lower part),
+// the multipliers M_rj = L_rj / L_jj above the diagonal (row j), 1/L_jj to sv and y to bv.
 __device__ __forceinline__ void chol_factor_diag(double (*Pm)[kPLD], double* bv, double* sv, double* xc, int c0,
                                                  int nsb, int* sfail) {
   const int lane = threadIdx.x & 31, rr = lane & 15, hh = lane >> 4;
@@ -1607,42 +1611,81 @@ __device__ __forceinline__ void chol_factor_diag(double (*Pm)[kPLD], double* bv,
   }
   double bb = (hh == 0 && rr < nsb) ? bv[c0 + rr] : 0.0;
   double cfac = 1.0;
+  // per own column k = 8 hh + q: cd_k and f_k; for the own row: cd, f and b' at its step
+  double cq[8], fq[8], my_cd = 1.0, my_f = 1.0, my_b = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) cq[q] = fq[q] = 1.0;
   bool ok = true;
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
+  for (int j = 0; j < 16; j += 2) {
     const int hj = j >> 3, qj = j & 7;
-    double* col = xc + (j & 1) * 20;
-    if (hh == hj) col[rr] = a[qj];
-    if (lane == j) col[16] = bb;
+    double* col = xc + ((j >> 1) & 1) * 36;   // [0,16) u, [16,32) v, [32] b_j, [33] b_j+1
+    if (hh == hj) {
+      col[rr] = a[qj];
+      col[16 + rr] = a[qj + 1];
+    }
+    if (lane == j || lane == j + 1) col[32 + lane - j] = bb;
     __syncwarp();
-    const double piv = col[j], colr = col[rr], bj = col[16];
-    double colk[8];
+    const double p = col[j], q = col[j + 1], s = col[16 + j + 1];
+    const double ur = col[rr], vr = col[16 + rr];
+    const double2 bjj = *reinterpret_cast<const double2*>(&col[32]);
+    double uk[8], vk[8];
 #pragma unroll
-    for (int q = 0; q < 8; q += 2) {
-      const double2 v = *reinterpret_cast<const double2*>(&col[8 * hh + q]);
-      colk[q] = v.x;
-      colk[q + 1] = v.y;
+    for (int t = 0; t < 8; t += 2) {
+      const double2 x = *reinterpret_cast<const double2*>(&col[8 * hh + t]);
+      const double2 y = *reinterpret_cast<const double2*>(&col[16 + 8 * hh + t]);
+      uk[t] = x.x;
+      uk[t + 1] = x.y;
+      vk[t] = y.x;
+      vk[t + 1] = y.y;
     }
-    ok = ok && (piv > 0.0);
-    const long long bits = __double_as_longlong(piv);
-    const double sc = __longlong_as_double((2046LL - ((bits >> 52) & 0x7FF)) << 52);   // 2^-E_j
+    const double det = fma(p, s, -(q * q));
+    ok = ok && (p > 0.0) && (det > 0.0);
+    const long long bits = __double_as_longlong(det);
+    const double sc = __longlong_as_double((2046LL - ((bits >> 52) & 0x7FF)) << 52);   // 2^-E
+    const double w1 = fma(s, ur, -(q * vr)), w2 = fma(p, vr, -(q * ur));
+    const double dets = det * sc, w1s = w1 * sc, w2s = w2 * sc;
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (8 * hh + q > j) a[q] = fma(a[q], piv, -(colr * colk[q])) * sc;
-    if (hh == 0 && rr > j) bb = fma(bb, piv, -(colr * bj)) * sc;
-    // column j is final
-    const double cdj = cfac * piv;
-    const double s = rsqrt(cdj);
-    const double linv = cfac * s;
-    cfac = cdj * sc;
-    if (hh == hj && rr >= j && rr < nsb) {
-      const double l = colr * s;
-      Pm[c0 + rr][c0 + j] = l;
-      if (rr > j) Pm[c0 + j][c0 + rr] = l * linv;
+    for (int t = 0; t < 8; ++t)
+      if (8 * hh + t > j + 1) a[t] = fma(a[t], dets, -fma(w1s, uk[t], w2s * vk[t]));
+    const double bj1 = fma(p, bjj.y, -(q * bjj.x));
+    if (hh == 0 && rr > j + 1) bb = fma(bb, dets, -fma(w1s, bjj.x, w2s * bjj.y));
+    // columns j, j+1 are final: only registers are written here
+    const double cp = cfac * p, cpd = cp * det;
+    if (hh == hj) {
+      a[qj + 1] = w2;
+      cq[qj] = cp;
+      fq[qj] = cfac;
+      cq[qj + 1] = cpd;
+      fq[qj + 1] = cp;
     }
-    if (lane == j && j < nsb) {
-      sv[c0 + j] = linv;
-      bv[c0 + j] = bj * s;
+    if (rr == j) {
+      my_cd = cp;
+      my_f = cfac;
+      my_b = bjj.x;
+    }
+    if (rr == j + 1) {
+      my_cd = cpd;
+      my_f = cp;
+      my_b = bj1;
+    }
+    cfac *= dets;
+  }
+  if (rr < nsb) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * hh + q;
+      if (k <= rr) {
+        const double s = rsqrt(cq[q]);
+        const double l = a[q] * s;
+        Pm[c0 + rr][c0 + k] = l;
+        if (k < rr) Pm[c0 + k][c0 + rr] = l * (fq[q] * s);
+      }
+    }
+    if (hh == 0) {
+      const double s = rsqrt(my_cd);
+      sv[c0 + rr] = my_f * s;
+      bv[c0 + rr] = my_b * s;
     }
   }
   if (lane == 0 && !ok) *sfail = 1;
@@ -1659,8 +1702,8 @@ __device__ bool chol_panel(int n, int kb, int t, double* __restrict__ A, double*
   double (*Pm)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);   // [128][kPLD]: D rows, then X rows
   double* bv = csm + 128 * kPLD;                                   // [128]
   double* sv = bv + 128;                                           // [64] 1/L_jj
-  double* xc = sv + 64;                                            // [40] column exchange of (b)
-  int* sfail = reinterpret_cast<int*>(xc + 40);
+  double* xc = sv + 64;                                            // [72] column exchange of (b)
+  int* sfail = reinterpret_cast<int*>(xc + 72);
   __syncthreads();
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
@@ -2139,7 +2182,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   if (n == 0) return HS2_OK;
   HS2_PROF("ba_cholesky", s);
   const int nbk = (n + kNB - 1) / kNB;
-  const size_t smem = sizeof(double) * (128 * kPLD + 128 + 64 + 40 + 2);   // panel (tile, backward need less)
+  const size_t smem = sizeof(double) * (128 * kPLD + 128 + 64 + 72 + 2);   // panel (tile, backward need less)
   static int grid_cap[64] = {0};
   int dev = 0;
   HS2_CUDA(cudaGetDevice(&dev));
