@@ -43,6 +43,9 @@ SIGNATURES = {
     "hs2_ba_reduced_system": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32,
                               _i32, _p, _p, _p, _p, _sz, _p],
     "hs2_ba_set_schur_path": [_i32],
+    "hs2_pgba_workspace_size": [_i64, _i64, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_sz)],
+    "hs2_pgba": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32,
+                 _i32, _f32, _f32, _p, _p, _i64, _p, _p, _sz, _p],
     "hs2_iproj": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p],
     "hs2_proj_trans": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _p, _i64, _i64, _p, _p, _p, _p],
     "hs2_bi_inter": [_p, _i64, _i32, _i32, _p, _i32, _i32, _p, _p, _p, _p],

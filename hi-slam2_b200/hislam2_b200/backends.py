@@ -133,6 +133,75 @@ def ba(poses, disps, intrinsics, *args, disps_sens=None):
     return [dx, None if motion_only else dz[:M], None]
 
 
+def pgba_workspace_bytes(num_poses, num_disps, ht, wd, num_edges, t0, t1):
+    n = ctypes.c_size_t(0)
+    _lib.check(_lib.load().hs2_pgba_workspace_size(num_poses, num_disps, ht, wd, num_edges, t0, t1,
+                                                   ctypes.byref(n)), "pgba_workspace_size")
+    return n.value
+
+
+def pgba(poses, disps, intrinsics, targets, weights, eta, Hsp, vsp, ii, jj, iip, jjp, t0, t1, lm, ep):
+    """Sim3 pose-graph bundle adjustment, ``droid_backends.pgba`` (reference
+    ``src/droid.cpp:171-196``): one damped Gauss-Newton step -> ``[dx, dz]``.
+
+    ``poses`` [N, 8] (t, q xyzw, s) are not modified (``dx`` [t1-t0, 7] is for the
+    caller's Sim3 retraction, as ``hislam2/depth_video.py:cuda_pgba`` does);
+    ``disps`` is updated in place.  ``Hsp`` [4, ..., Np, 7, 7] and ``vsp`` [2, ..., Np, 7]
+    are the relative-pose factors at ``iip`` / ``jjp`` (``pgo_buffer.py``'s
+    ``global_relative_posesim3_constraints`` layout).
+    """
+    for name, t in (("poses", poses), ("disps", disps), ("ii", ii), ("jj", jj)):
+        _contig(name, t)
+    dev = poses.device
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("targets", targets),
+                    ("weights", weights), ("eta", eta), ("Hsp", Hsp), ("vsp", vsp), ("ii", ii), ("jj", jj),
+                    ("iip", iip), ("jjp", jjp)):
+        _cuda(name, t, dev)
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics), ("targets", targets),
+                    ("weights", weights), ("eta", eta), ("Hsp", Hsp), ("vsp", vsp)):
+        _dtype(name, t, torch.float32)
+    for name, t in (("ii", ii), ("jj", jj), ("iip", iip), ("jjp", jjp)):
+        _dtype(name, t, torch.int64)
+    if poses.dim() != 2 or poses.shape[1] != 8:
+        raise RuntimeError("poses must be [N, 8] Sim3 (got %s)" % tuple(poses.shape))
+    if disps.dim() != 3:
+        raise RuntimeError("disps must be [N, H, W] (got %s)" % tuple(disps.shape))
+    if intrinsics.numel() < 4:
+        raise RuntimeError("intrinsics must hold fx, fy, cx, cy")
+    E, Np = ii.numel(), iip.numel()
+    ht, wd = disps.shape[1], disps.shape[2]
+    if jj.numel() != E or jjp.numel() != Np:
+        raise RuntimeError("ii/jj and iip/jjp must have matching lengths")
+    for name, t in (("targets", targets), ("weights", weights)):
+        if tuple(t.shape) != (E, 2, ht, wd):
+            raise RuntimeError("%s must be [num_edges, 2, H, W] = %s (got %s)" % (name, (E, 2, ht, wd),
+                                                                                 tuple(t.shape)))
+    if Hsp.numel() != 4 * Np * 49 or vsp.numel() != 2 * Np * 7:
+        raise RuntimeError("Hsp must hold 4 x %d blocks 7x7 and vsp 2 x %d rows of 7 (got %s, %s)"
+                           % (Np, Np, tuple(Hsp.shape), tuple(vsp.shape)))
+    if eta.numel() % (ht * wd) != 0:
+        raise RuntimeError("eta must hold whole [H, W] maps (got %s)" % tuple(eta.shape))
+    targets, weights, eta = targets.contiguous(), weights.contiguous(), eta.contiguous()
+    Hsp, vsp, iip, jjp = Hsp.contiguous(), vsp.contiguous(), iip.contiguous(), jjp.contiguous()
+    intrinsics = intrinsics.contiguous()
+    t0, t1 = int(t0), int(t1)
+    K, Kd = poses.shape[0], disps.shape[0]
+    P = t1 - t0
+    ws_bytes = pgba_workspace_bytes(K, Kd, ht, wd, E, t0, t1)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    S = max(1, min(min(K, Kd), P + E))
+    dx = torch.zeros(max(P, 0), 7, dtype=torch.float32, device=dev)
+    dz = torch.zeros(S, ht * wd, dtype=torch.float32, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_pgba(
+        _ptr(poses), K, _ptr(disps), Kd, ht, wd, _ptr(intrinsics), _ptr(targets), _ptr(weights), _ptr(eta),
+        eta.numel() // (ht * wd), _ptr(Hsp), _ptr(vsp), _ptr(iip), _ptr(jjp), Np, _ptr(ii), _ptr(jj), E, t0, t1,
+        float(lm), float(ep), _ptr(dx), _ptr(dz), S, _ptr(info), _ptr(ws), ws_bytes, _stream(dev)), "pgba")
+    h = info.cpu()
+    _raise_device_errors(int(h[0]), "pgba")
+    return [dx, dz[:int(h[1])]]
+
+
 def ba_reduced_system(poses, disps, intrinsics, targets, weights, eta, ii, jj, t0, t1, motion_only=False):
     """The reduced camera system (A - S, b - v) of one linearisation at the given state,
     before damping, as float64 CUDA tensors ``[6P, 6P]`` and ``[6P]`` (diagnostic)."""

@@ -2464,3 +2464,580 @@ extern "C" int hs2_ba_set_schur_path(int path) {
   g_schur_path.store(path);
   return HS2_OK;
 }
+
+// ================================================================= pgba ===
+// Sim3 pose-graph bundle adjustment (reference operator: src/droid.cpp:171-196 ->
+// src/droid_kernels.cu:1940-2044): ONE damped Gauss-Newton step over Sim3 poses
+// [t(3), q(4), s] (7-dof tangent [tau, phi, sigma]) and per-pixel inverse depths, with
+// the caller's relative-pose factors added to the pose system.  Poses are not moved
+// (dx is returned for the caller's Sim3 retraction); disparities are updated in place.
+//
+//   keys        as for ba (ba_keys_kernel): depth frames kx, edge groups, row lists
+//   pg_edge     Gij = Gj Gi^-1 (Sim3) and the 7x7 map L with Ji = L Jj, L = -adjSim3
+//               as the reference writes it (:122-145; its rotation and scale columns
+//               are not the derivative of the reprojection, and are kept for parity)
+//   pg_linearize per (depth frame, pixel chunk): residuals and Sim3 Jacobians of every
+//               edge leaving the frame (:608-858): each edge's Hjj / vj summed in FP64,
+//               its E row written, the frame's Ei = sum L Eij row, Q = 1/(C + eta), w
+//   pg_assemble Hii = L Hjj L^T, Hij = L Hjj, vi = L vj into the FP64 system (keys - t0,
+//               negatives dropped: SparseBlock::update_lhs/update_rhs :1598-1638)
+//   pg_prior    the relative-pose blocks Hsp / vsp at iip, jjp (:2004-2013)
+//   pg_schur    per depth frame the Gram of its Schur rows weighted by Q, subtracted
+//               (schur_block + EEt6x6 + Ev6x1 at D = 7, :1466-1560, :1689-1779)
+//   cholesky    the BA kernel on the system padded to even order with an identity row
+//   pg_backsub  dz = Q (w - sum E.dx) with the reference's ix <= 0 skip, disps += dz
+// Only the lower triangle (with whole diagonal blocks) of the reduced matrix is
+// written and read, as the reference's SimplicialLLT reads it: a block at keys (R, C)
+// is added when R >= C.
+namespace hs2 {
+
+constexpr int kPgD = 7;
+constexpr int kPgTab = 72;        // floats per edge: t 0..2, q 3..6, s 7, L 8..56 (row-major), s R 57..65
+constexpr int kPgH = 35;          // upper triangle of Hjj (28), then vj (7)
+constexpr int kPgThreads = 256;
+constexpr int kPgPPT = 4;
+constexpr int kPgChunk = kPgThreads * kPgPPT;
+constexpr int kPgSplit = 8;       // CTAs per depth frame in the Gram
+
+__host__ __device__ __forceinline__ int64_t pg_order(int P) { return 7 * (int64_t)P + ((7 * (int64_t)P) & 1); }
+
+__device__ __forceinline__ int tri7(int r, int c) { return r * 7 - (r * (r - 1)) / 2 + (c - r); }
+
+__global__ void pg_edge_kernel(const float* __restrict__ poses, const int64_t* __restrict__ ii,
+                               const int64_t* __restrict__ jj, int E, float* __restrict__ ptab,
+                               double* __restrict__ L64, const int32_t* __restrict__ info) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gid / 7, c = gid - (gid / 7) * 7;
+  if (e >= E || info[0]) return;
+  const float* pi = poses + 8 * ii[e];
+  const float* pj = poses + 8 * jj[e];
+  const double ti[3] = {pi[0], pi[1], pi[2]}, qi[4] = {pi[3], pi[4], pi[5], pi[6]};
+  const double tj[3] = {pj[0], pj[1], pj[2]}, qj[4] = {pj[3], pj[4], pj[5], pj[6]};
+  double t_se3[3], q[4], rti[3];
+  relative_pose(ti, qi, tj, qj, t_se3, q);   // qij = qj conj(qi)
+  quat_rotate(q, ti, rti);
+  const double sij = (double)pj[7] / (double)pi[7];
+  const double t[3] = {tj[0] - sij * rti[0], tj[1] - sij * rti[1], tj[2] - sij * rti[2]};
+  float* tab = ptab + (int64_t)e * kPgTab;
+  if (c == 0) {
+    for (int k = 0; k < 3; ++k) tab[k] = (float)t[k];
+    for (int k = 0; k < 4; ++k) tab[3 + k] = (float)q[k];
+    tab[7] = (float)sij;
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - z * w),     2 * (x * z + y * w),
+                         2 * (x * y + z * w),     1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                         2 * (x * z - y * w),     2 * (y * z + x * w),     1 - 2 * (x * x + y * y)};
+    for (int k = 0; k < 9; ++k) tab[57 + k] = (float)(sij * R[k]);
+    for (int k = 66; k < kPgTab; ++k) tab[k] = 0.f;
+  }
+  // column c of L: Ji for Jj = unit vector c.  -adjSim3 (:122-145):
+  //   Ji[0:3] = s (-R^T a),  Ji[3:6] = s (-R^T (b + a x t)) - c6 t,  Ji[6] = -c6
+  double u[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) u[k] = k == c ? 1.0 : 0.0;
+  const double c6 = c == 6 ? 1.0 : 0.0;
+  double r[6];
+  pose_jacobian_i(t, q, u, r);
+  double col[7];
+  for (int k = 0; k < 3; ++k) col[k] = sij * r[k];
+  for (int k = 0; k < 3; ++k) col[3 + k] = sij * r[3 + k] - c6 * t[k];
+  col[6] = -c6;
+  for (int k = 0; k < 7; ++k) {
+    tab[8 + k * 7 + c] = (float)col[k];
+    L64[(int64_t)e * 49 + k * 7 + c] = col[k];
+  }
+}
+
+// One CTA per (depth frame slot, chunk of kPgChunk pixels); thread t owns the pixels
+// t + 256 k.  For every edge of the frame (in group order) each pixel is moved by
+// Gij, projected and linearised as the reference does per pixel (:700-814); the
+// edge's 35 Hessian sums are reduced over the CTA into FP64 accumulators.
+__global__ void __launch_bounds__(kPgThreads)
+pg_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
+                    const float* __restrict__ targets, const float* __restrict__ weights,
+                    const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj, int t0,
+                    int t1, const float* __restrict__ ptab, BaPtrs w, float* __restrict__ erows,
+                    float* __restrict__ qbuf, float* __restrict__ wbuf, double* __restrict__ hedge,
+                    const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const int f = w.kx[s];
+  const bool inwin = f >= t0 && f < t1;
+  const size_t HWs = (size_t)row_stride(HW);
+  __shared__ float tab[kPgTab];
+  __shared__ float red[kPgThreads / 32][kPgH];
+  const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
+  const int base = blockIdx.y * kPgChunk + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float xn[kPgPPT], yn[kPgPPT], hd[kPgPPT], C[kPgPPT], W[kPgPPT], Ei[kPgPPT][kPgD];
+#pragma unroll
+  for (int k = 0; k < kPgPPT; ++k) {
+    const int p = base + k * kPgThreads;
+    const bool ok = p < HW;
+    xn[k] = ok ? ((float)(p % wd) - cx) / fx : 0.f;
+    yn[k] = ok ? ((float)(p / wd) - cy) / fy : 0.f;
+    hd[k] = ok ? disps[(int64_t)f * HW + p] : 0.f;
+    C[k] = 0.f;
+    W[k] = 0.f;
+#pragma unroll
+    for (int d = 0; d < kPgD; ++d) Ei[k][d] = 0.f;
+  }
+  for (int g = w.gptr[s]; g < w.gptr[s + 1]; ++g) {
+    const int e = w.gedge[g];
+    __syncthreads();   // tab / red of the previous edge are consumed
+    if (threadIdx.x < kPgTab) tab[threadIdx.x] = ptab[(int64_t)e * kPgTab + threadIdx.x];
+    __syncthreads();
+    const bool self = jj[e] == (int64_t)f;
+    const size_t row = (size_t)w.epos[e];
+    const float* tg = targets + (int64_t)e * 2 * HW;
+    const float* wg = weights + (int64_t)e * 2 * HW;
+    float h[kPgH];
+#pragma unroll
+    for (int i = 0; i < kPgH; ++i) h[i] = 0.f;
+#pragma unroll
+    for (int k = 0; k < kPgPPT; ++k) {
+      const int p = base + k * kPgThreads;
+      if (p >= HW) continue;
+      // Xj = s R X + h t with X = (xn, yn, 1) (actSim3 :96-102)
+      const float x = tab[57] * xn[k] + tab[58] * yn[k] + tab[59] + hd[k] * tab[0];
+      const float y = tab[60] * xn[k] + tab[61] * yn[k] + tab[62] + hd[k] * tab[1];
+      const float Z = tab[63] * xn[k] + tab[64] * yn[k] + tab[65] + hd[k] * tab[2];
+      const float hh = hd[k];
+      const bool bad = Z < kMinDepth;
+      const float z = bad ? 0.f : Z;
+      const float dd = bad ? 0.f : 1.f / Z;
+      const float d2 = dd * dd;
+      float wu = bad ? 0.f : 0.001f * wg[p];
+      float wv = bad ? 0.f : 0.001f * wg[HW + p];
+      const float ru = tg[p] - (fx * (x / Z) + cx);
+      const float rv = tg[HW + p] - (fy * (y / Z) + cy);
+      const float Jp0 = fx * dd, Jp2 = fx * (-x * d2), Jp4 = fy * dd, Jp5 = fy * (-y * d2);
+      const float Jzu = Jp0 * tab[0] + Jp2 * tab[2];
+      const float Jzv = Jp4 * tab[1] + Jp5 * tab[2];
+      C[k] += wu * Jzu * Jzu + wv * Jzv * Jzv;
+      W[k] += wu * ru * Jzu + wv * rv * Jzv;
+      if (self) {
+        wu = 0.f;
+        wv = 0.f;
+      }
+      // Jj rows of u and v (:733-740, :767-774; Jp[1] = Jp[3] = 0)
+      const float Ju[kPgD] = {Jp0 * hh, 0.f, Jp2 * hh, Jp2 * y, Jp0 * z - Jp2 * x, -Jp0 * y, Jp0 * x + Jp2 * z};
+      const float Jv[kPgD] = {0.f, Jp4 * hh, Jp5 * hh, -Jp4 * z + Jp5 * y, -Jp5 * x, Jp4 * x, Jp4 * y + Jp5 * z};
+#pragma unroll
+      for (int a = 0; a < kPgD; ++a) {
+#pragma unroll
+        for (int b = a; b < kPgD; ++b) h[tri7(a, b)] += wu * Ju[a] * Ju[b] + wv * Jv[a] * Jv[b];
+        h[28 + a] += wu * ru * Ju[a] + wv * rv * Jv[a];
+      }
+      float ej[kPgD];
+#pragma unroll
+      for (int a = 0; a < kPgD; ++a) {
+        ej[a] = wu * Jzu * Ju[a] + wv * Jzv * Jv[a];
+        erows[(row * kPgD + a) * HWs + p] = ej[a];
+      }
+      if (inwin) {
+#pragma unroll
+        for (int r = 0; r < kPgD; ++r) {
+          float acc = 0.f;
+#pragma unroll
+          for (int c = 0; c < kPgD; ++c) acc += tab[8 + r * 7 + c] * ej[c];
+          Ei[k][r] += acc;
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kPgH; ++i) {
+      const float v = warp_sum(h[i]);
+      if (lane == 0) red[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kPgH) {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < kPgThreads / 32; ++q) acc += (double)red[q][threadIdx.x];
+      atomicAdd(&hedge[(int64_t)e * kPgH + threadIdx.x], acc);
+    }
+  }
+  const int64_t er = eta_rows == 1 ? 0 : s;
+  const size_t wrow = inwin ? (size_t)w.wpos[f - t0] : 0;
+#pragma unroll
+  for (int k = 0; k < kPgPPT; ++k) {
+    const int p = base + k * kPgThreads;
+    if (p >= HW) continue;
+    qbuf[(int64_t)s * HW + p] = 1.f / (C[k] + eta[er * HW + p]);
+    wbuf[(int64_t)s * HW + p] = W[k];
+    if (inwin) {
+#pragma unroll
+      for (int d = 0; d < kPgD; ++d) erows[(wrow * kPgD + d) * HWs + p] = Ei[k][d];
+    }
+  }
+}
+
+// Adds row r of a 7x7 block to the system at block keys (R, C) when R >= C (lower
+// triangle with whole diagonal blocks); negative keys are dropped.
+__device__ __forceinline__ void pg_add_row(double* A, int64_t npad, int R, int C, int r, const double* v) {
+  if (R < 0 || C < 0 || R < C) return;
+  double* dst = A + (7 * (int64_t)R + r) * npad + 7 * (int64_t)C;
+#pragma unroll
+  for (int c = 0; c < kPgD; ++c) atomicAdd(dst + c, v[c]);
+}
+
+// Seven threads per edge, thread r forms row r of Hii, Hij, Hji^T's column and Hjj.
+__global__ void pg_assemble_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, int E, int t0,
+                                   int64_t npad, const double* __restrict__ L64, const double* __restrict__ hedge,
+                                   double* __restrict__ A, double* __restrict__ b, const int32_t* __restrict__ info) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gid / 7, r = gid - (gid / 7) * 7;
+  if (e >= E || info[0]) return;
+  const int i = (int)(ii[e] - t0), j = (int)(jj[e] - t0);
+  const double* H = hedge + (int64_t)e * kPgH;
+  const double* L = L64 + (int64_t)e * 49;
+  double hjj_r[kPgD], hij_r[kPgD], hii_r[kPgD];
+#pragma unroll
+  for (int c = 0; c < kPgD; ++c) hjj_r[c] = H[r <= c ? tri7(r, c) : tri7(c, r)];
+  double vi = 0.0;
+#pragma unroll
+  for (int c = 0; c < kPgD; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPgD; ++k) acc += L[r * 7 + k] * H[k <= c ? tri7(k, c) : tri7(c, k)];
+    hij_r[c] = acc;
+    vi += L[r * 7 + c] * H[28 + c];
+  }
+#pragma unroll
+  for (int c = 0; c < kPgD; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPgD; ++k) acc += hij_r[k] * L[c * 7 + k];
+    hii_r[c] = acc;
+  }
+  pg_add_row(A, npad, i, i, r, hii_r);
+  pg_add_row(A, npad, i, j, r, hij_r);
+  pg_add_row(A, npad, j, j, r, hjj_r);
+  // Hji = Hij^T: row r of Hij is column r of the block at (j, i)
+  if (j >= 0 && i >= 0 && j >= i) {
+    double* dst = A + 7 * (int64_t)j * npad + 7 * (int64_t)i + r;
+#pragma unroll
+    for (int c = 0; c < kPgD; ++c) atomicAdd(dst + c * npad, hij_r[c]);
+  }
+  if (i >= 0) atomicAdd(&b[7 * (int64_t)i + r], vi);
+  if (j >= 0) atomicAdd(&b[7 * (int64_t)j + r], H[28 + r]);
+}
+
+// Seven threads per relative-pose factor p: blocks Hsp[0..3][p] at (iip,iip), (iip,jjp),
+// (jjp,iip), (jjp,jjp) and vsp[0..1][p] at iip, jjp.  Keys >= t1 are refused.
+__global__ void pg_prior_kernel(const float* __restrict__ Hsp, const float* __restrict__ vsp,
+                                const int64_t* __restrict__ iip, const int64_t* __restrict__ jjp, int64_t Np,
+                                int t0, int t1, int64_t npad, double* __restrict__ A, double* __restrict__ b,
+                                int32_t* __restrict__ info) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = gid / 7;
+  const int r = (int)(gid - p * 7);
+  if (p >= Np || info[0]) return;
+  const int64_t a = iip[p], c = jjp[p];
+  if (a >= t1 || c >= t1) {
+    atomicOr(info, HS2_DEV_BAD_INDEX);
+    return;
+  }
+  const int i = a < t0 ? -1 : (int)(a - t0), j = c < t0 ? -1 : (int)(c - t0);
+  const int keys[4][2] = {{i, i}, {i, j}, {j, i}, {j, j}};
+  for (int blk = 0; blk < 4; ++blk) {
+    const float* src = Hsp + ((int64_t)blk * Np + p) * 49 + r * 7;
+    double v[kPgD];
+#pragma unroll
+    for (int k = 0; k < kPgD; ++k) v[k] = (double)src[k];
+    pg_add_row(A, npad, keys[blk][0], keys[blk][1], r, v);
+  }
+  if (i >= 0) atomicAdd(&b[7 * (int64_t)i + r], (double)vsp[p * 7 + r]);
+  if (j >= 0) atomicAdd(&b[7 * (int64_t)j + r], (double)vsp[(Np + p) * 7 + r]);
+}
+
+__global__ void pg_pad_kernel(double* __restrict__ A, int64_t n, int64_t npad) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && npad > n) A[n * npad + n] = 1.0;
+}
+
+// Gram of a frame's Schur rows (stored at rptr[s] + a, a < nr, in srow order): 32 x 32 output tiles of the (7 R) x (7 R) matrix
+// G_xy = sum_p E_x Q E_y, lower tiles only, tiles spread over gridDim.y CTAs.  Each
+// unordered pair {x, y} of the full Gram is subtracted once at the lower-triangle
+// position of the system it maps to (twice onto a diagonal entry hit by both orders).
+__global__ void __launch_bounds__(256)
+pg_schur_kernel(int HW, int64_t npad, BaPtrs w, const float* __restrict__ erows, const float* __restrict__ qbuf,
+                double* __restrict__ A, const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const int r0 = w.sptr[s], nr = w.sptr[s + 1] - r0;
+  const size_t rbase = (size_t)w.rptr[s];   // storage position of the frame's first Schur row
+  const int m = kPgD * nr, nt = (m + 31) / 32, T = nt * (nt + 1) / 2;
+  const size_t HWs = (size_t)row_stride(HW);
+  __shared__ float Xs[32][33], Ys[32][33];
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const float* Q = qbuf + (int64_t)s * HW;
+  for (int t = blockIdx.y; t < T; t += gridDim.y) {
+    int ti = 0;
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    const int tj = t - ti * (ti + 1) / 2;
+    float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    for (int p0 = 0; p0 < HW; p0 += 32) {
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int idx = tid + q * 256, rl = idx >> 5, pc = idx & 31, p = p0 + pc;
+        const int x = 32 * ti + rl, y = 32 * tj + rl;
+        float vx = 0.f, vy = 0.f;
+        if (p < HW && x < m) {
+          const size_t row = rbase + x / kPgD;
+          vx = erows[(row * kPgD + x % kPgD) * HWs + p] * Q[p];
+        }
+        if (p < HW && y < m) {
+          const size_t row = rbase + y / kPgD;
+          vy = erows[(row * kPgD + y % kPgD) * HWs + p];
+        }
+        Xs[rl][pc] = vx;
+        Ys[rl][pc] = vy;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) {
+        const float a0 = Xs[ty][k], a1 = Xs[ty + 16][k], b0 = Ys[tx][k], b1 = Ys[tx + 16][k];
+        acc[0][0] += a0 * b0;
+        acc[0][1] += a0 * b1;
+        acc[1][0] += a1 * b0;
+        acc[1][1] += a1 * b1;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int x = 32 * ti + ty + 16 * u, y = 32 * tj + tx + 16 * v;
+        if (x >= m || y >= m || (ti == tj && x < y)) continue;
+        const double g = (double)acc[u][v];
+        const int ax = x / kPgD, dx = x % kPgD, ay = y / kPgD, dy = y % kPgD;
+        const int64_t pa = w.spose[r0 + ax], pb = w.spose[r0 + ay];
+        const int64_t gx = 7 * pa + dx, gy = 7 * pb + dy;
+        if (x == y) atomicAdd(&A[gx * npad + gy], -g);
+        else if (gx > gy) atomicAdd(&A[gx * npad + gy], -g);
+        else if (gy > gx) atomicAdd(&A[gy * npad + gx], -g);
+        else atomicAdd(&A[gx * npad + gy], -2.0 * g);
+      }
+  }
+}
+
+// b -= E.(Q w) for every Schur row (Ev6x1 :1525-1560); one warp per (row, plane).
+__global__ void __launch_bounds__(256)
+pg_schur_rhs_kernel(int HW, BaPtrs w, const float* __restrict__ erows, const float* __restrict__ qbuf,
+                    const float* __restrict__ wbuf, double* __restrict__ b, const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const int r0 = w.sptr[s], nr = w.sptr[s + 1] - r0;
+  const size_t HWs = (size_t)row_stride(HW);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float* Q = qbuf + (int64_t)s * HW;
+  const float* Wv = wbuf + (int64_t)s * HW;
+  for (int task = warp; task < nr * kPgD; task += 8) {
+    const int a = task / kPgD, d = task % kPgD;
+    const float* e = erows + ((size_t)(w.rptr[s] + a) * kPgD + d) * HWs;
+    float acc = 0.f;
+    for (int p = lane; p < HW; p += 32) acc += e[p] * (Q[p] * Wv[p]);
+    acc = warp_sum(acc);
+    if (lane == 0) atomicAdd(&b[7 * (int64_t)w.spose[r0 + a] + d], -(double)acc);
+  }
+}
+
+// dz = Q (w - sum_rows E.dx[pose]) over the frame's rows whose pose index lies in
+// (0, P) (EvT6x1_kernel :1562-1582 skips ix <= 0), disps[kx] += dz (:1398-1411).
+__global__ void __launch_bounds__(kPgThreads)
+pg_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const float* __restrict__ erows,
+                  const float* __restrict__ qbuf, const float* __restrict__ wbuf, const float* __restrict__ dx,
+                  float* __restrict__ dz, const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const size_t HWs = (size_t)row_stride(HW);
+  const int r0 = w.rptr[s], r1 = w.rptr[s + 1];
+  const int f = w.kx[s];
+  const int base = blockIdx.y * kPgChunk + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < kPgPPT; ++k) {
+    const int p = base + k * kPgThreads;
+    if (p >= HW) continue;
+    float acc = 0.f;
+    for (int r = r0; r < r1; ++r) {
+      const int pose = w.rpose[r];
+      if (pose <= 0 || pose >= P) continue;
+      const float* e = erows + (size_t)r * kPgD * HWs + p;
+      float dw = 0.f;
+#pragma unroll
+      for (int d = 0; d < kPgD; ++d) dw += e[d * HWs] * dx[7 * pose + d];
+      acc += dw;
+    }
+    const float v = qbuf[(int64_t)s * HW + p] * (wbuf[(int64_t)s * HW + p] - acc);
+    dz[(int64_t)s * HW + p] = v;
+    disps[(int64_t)f * HW + p] += v;
+  }
+}
+
+struct PgLayout {
+  BaLayout k;   // key arrays (the other fields are unused)
+  size_t ptab, L64, hedge, erows, qbuf, wbuf, A, b, x, dxf, L11, dinv, ychol, ctl, total;
+};
+
+static PgLayout pg_layout(int64_t K, int HW, int64_t E, int P) {
+  PgLayout L;
+  std::memset(&L, 0, sizeof(L));
+  const int64_t R = P + E;
+  const int64_t S = std::min<int64_t>(K, R);
+  const int64_t n = pg_order(P);
+  const int64_t nbk = (n + kNB - 1) / kNB;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o = align256(o + bytes); return at; };
+  L.k.flag = take(sizeof(int) * (K + 1));
+  L.k.slot = take(sizeof(int) * (K + 1));
+  L.k.kx = take(sizeof(int) * (S + 1));
+  L.k.gptr = take(sizeof(int) * (S + 2));
+  L.k.gedge = take(sizeof(int) * (E + 1));
+  L.k.cursor = take(sizeof(int) * (S + 1));
+  L.k.rptr = take(sizeof(int) * (S + 2));
+  L.k.rrow = take(sizeof(int) * (R + 1));
+  L.k.rpose = take(sizeof(int) * (R + 1));
+  L.k.sptr = take(sizeof(int) * (S + 2));
+  L.k.srow = take(sizeof(int) * (R + 1));
+  L.k.spose = take(sizeof(int) * (R + 1));
+  L.k.epos = take(sizeof(int) * (E + 1));
+  L.k.wpos = take(sizeof(int) * (P + 1));
+  L.ptab = take(sizeof(float) * kPgTab * (E + 1));
+  L.L64 = take(sizeof(double) * 49 * (E + 1));
+  L.hedge = take(sizeof(double) * kPgH * (E + 1));
+  L.erows = take(sizeof(float) * kPgD * (size_t)R * row_stride(HW));
+  L.qbuf = take(sizeof(float) * (size_t)S * HW);
+  L.wbuf = take(sizeof(float) * (size_t)S * HW);
+  L.A = take(sizeof(double) * (size_t)(n * n + 1));
+  L.b = take(sizeof(double) * (size_t)(n + 1));
+  L.x = take(sizeof(double) * (size_t)(n + 1));
+  L.dxf = take(sizeof(float) * (size_t)(n + 1));
+  L.L11 = take(sizeof(double) * (size_t)nbk * kNB * kNB);
+  L.dinv = take(sizeof(double) * (size_t)nbk * kNB);
+  L.ychol = take(sizeof(double) * (size_t)(n + 1));
+  L.ctl = take(sizeof(unsigned) * (4 + 2 * (size_t)nbk));
+  L.total = o;
+  return L;
+}
+
+}  // namespace hs2
+
+extern "C" int hs2_pgba_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd, int64_t num_edges,
+                                       int t0, int t1, size_t* bytes) {
+  using namespace hs2;
+  if (!bytes) {
+    set_error("pgba_workspace_size: null output");
+    return HS2_ERR_INVALID;
+  }
+  BaProblem p = make_problem(num_poses, num_disps, ht, wd, num_edges, t0, t1, 0);
+  int rc = ba_check(p, "pgba_workspace_size");
+  if (rc) return rc;
+  *bytes = pg_layout(p.K, p.HW, p.E, p.P).total;
+  return HS2_OK;
+}
+
+extern "C" int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int64_t num_disps, int ht, int wd,
+                        const float* intrinsics, const float* targets, const float* weights, const float* eta,
+                        int64_t eta_rows, const float* Hsp, const float* vsp, const int64_t* iip,
+                        const int64_t* jjp, int64_t num_factors, const int64_t* ii, const int64_t* jj,
+                        int64_t num_edges, int t0, int t1, float lm, float ep, float* dx, float* dz,
+                        int64_t dz_rows, int32_t* info, void* workspace, size_t workspace_bytes,
+                        hs2_stream_t stream) {
+  using namespace hs2;
+  BaProblem p = make_problem(num_poses, num_disps, ht, wd, num_edges, t0, t1, 0);
+  int rc = ba_check(p, "pgba");
+  if (rc) return rc;
+  const int P = p.P;
+  const int64_t S = std::min<int64_t>(p.K, (int64_t)P + p.E);
+  if (eta_rows <= 0) {
+    set_error("pgba: eta must have at least one row");
+    return HS2_ERR_INVALID;
+  }
+  if (num_factors < 0 || num_factors > (1 << 24) || (num_factors > 0 && (!Hsp || !vsp || !iip || !jjp))) {
+    set_error("pgba: bad relative-pose factors (count %lld)", (long long)num_factors);
+    return HS2_ERR_INVALID;
+  }
+  if (dz_rows < S) {
+    set_error("pgba: dz needs at least %lld rows (got %lld)", (long long)S, (long long)dz_rows);
+    return HS2_ERR_INVALID;
+  }
+  const PgLayout L = pg_layout(p.K, p.HW, p.E, P);
+  if (!workspace || workspace_bytes < L.total) {
+    set_error("pgba: workspace of %zu bytes required (got %zu)", L.total, workspace_bytes);
+    return HS2_ERR_WORKSPACE;
+  }
+  if ((rc = bind_device(disps))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  char* wsb = static_cast<char*>(workspace);
+  BaPtrs w = ba_ptrs(workspace, L.k);
+  float* ptab = (float*)(wsb + L.ptab);
+  double* L64 = (double*)(wsb + L.L64);
+  double* hedge = (double*)(wsb + L.hedge);
+  float* erows = (float*)(wsb + L.erows);
+  float* qbuf = (float*)(wsb + L.qbuf);
+  float* wbuf = (float*)(wsb + L.wbuf);
+  float* dxf = (float*)(wsb + L.dxf);
+  w.A = (double*)(wsb + L.A);
+  w.b = (double*)(wsb + L.b);
+  w.x = (double*)(wsb + L.x);
+  CholBuf cb{(double*)(wsb + L.L11), (double*)(wsb + L.dinv), (double*)(wsb + L.ychol), (unsigned*)(wsb + L.ctl)};
+  const int E = (int)p.E;
+  const int64_t n = 7 * (int64_t)P, npad = pg_order(P);
+  const int nchunk = (p.HW + kPgChunk - 1) / kPgChunk;
+
+  if ((rc = run_keys(p, ii, jj, eta_rows, w, info, s))) return rc;
+  if (E > 0) {
+    HS2_PROF("pg_edge", s);
+    pg_edge_kernel<<<(7 * E + 127) / 128, 128, 0, s>>>(poses, ii, jj, E, ptab, L64, info);
+    HS2_LAUNCH_CHECK("pg_edge_kernel");
+    HS2_CUDA(cudaMemsetAsync(hedge, 0, sizeof(double) * kPgH * (size_t)E, s));
+  }
+  if (P > 0) {
+    HS2_CUDA(cudaMemsetAsync(w.A, 0, sizeof(double) * (size_t)(npad * npad), s));
+    HS2_CUDA(cudaMemsetAsync(w.b, 0, sizeof(double) * (size_t)npad, s));
+    pg_pad_kernel<<<1, 32, 0, s>>>(w.A, n, npad);
+    HS2_LAUNCH_CHECK("pg_pad_kernel");
+  }
+  if (S > 0) {
+    HS2_PROF("pg_linearize", s);
+    pg_linearize_kernel<<<dim3((unsigned)S, nchunk), kPgThreads, 0, s>>>(
+        disps, p.HW, p.wd, intrinsics, targets, weights, eta, eta_rows, jj, t0, t1, ptab, w, erows, qbuf, wbuf, hedge,
+        info);
+    HS2_LAUNCH_CHECK("pg_linearize_kernel");
+  }
+  if (E > 0 && P > 0) {
+    HS2_PROF("pg_assemble", s);
+    pg_assemble_kernel<<<(7 * E + 127) / 128, 128, 0, s>>>(ii, jj, E, t0, npad, L64, hedge, w.A, w.b, info);
+    HS2_LAUNCH_CHECK("pg_assemble_kernel");
+  }
+  if (num_factors > 0) {
+    HS2_PROF("pg_prior", s);
+    pg_prior_kernel<<<(unsigned)((7 * num_factors + 127) / 128), 128, 0, s>>>(Hsp, vsp, iip, jjp, num_factors, t0,
+                                                                              t1, npad, w.A, w.b, info);
+    HS2_LAUNCH_CHECK("pg_prior_kernel");
+  }
+  if (P > 0 && S > 0) {
+    HS2_PROF("pg_schur", s);
+    pg_schur_kernel<<<dim3((unsigned)S, kPgSplit), 256, 0, s>>>(p.HW, npad, w, erows, qbuf, w.A, info);
+    HS2_LAUNCH_CHECK("pg_schur_kernel");
+    pg_schur_rhs_kernel<<<(unsigned)S, 256, 0, s>>>(p.HW, w, erows, qbuf, wbuf, w.b, info);
+    HS2_LAUNCH_CHECK("pg_schur_rhs_kernel");
+  }
+  if (P > 0) {
+    if ((rc = run_cholesky((int)npad, lm, ep, w, cb, dxf, info, s))) return rc;
+    HS2_CUDA(cudaMemcpyAsync(dx, dxf, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  }
+  if (S > 0) {
+    HS2_PROF("pg_backsub", s);
+    pg_backsub_kernel<<<dim3((unsigned)S, nchunk), kPgThreads, 0, s>>>(disps, p.HW, P, w, erows, qbuf, wbuf, dxf,
+                                                                       dz, info);
+    HS2_LAUNCH_CHECK("pg_backsub_kernel");
+  }
+  return HS2_OK;
+}

@@ -192,3 +192,39 @@ def make_corr_problem(name="frontend", seed=0, device="cpu", num_edges=None, dty
     return dict(fmaps=fmaps.to(device=device, dtype=dtype), ii=ii.to(device), jj=jj.to(device),
                 coords=coords.to(device=device, dtype=torch.float32), radius=cfg["radius"],
                 num_levels=num_levels)
+
+
+def make_pgba_problem(name="frontend_small", seed=0, device="cpu", num_factors=None, scale_sigma=0.05,
+                      info_range=(3.0, 6.0)):
+    """Inputs of ``droid_backends.pgba`` for workload ``name``: the BA problem of the same
+    name with Sim3 poses [K, 8] (scale exp(N(0, scale_sigma)) appended) and
+    ``num_factors`` (default 2K) relative-pose factors between random frames below t1,
+    about a quarter of them touching frames before t0.  Each factor has Jacobians
+    Ji, Jj ~ N(0, 1) (7x7), information diag(10^U(info_range)), weight pw = 1e-3 and
+    residual r ~ N(0, 0.01): Hsp = pw [Ji' W Ji, Ji' W Jj, Jj' W Ji, Jj' W Jj]
+    [4, 1, Np, 7, 7] and vsp = -pw [Ji' W r, Jj' W r] [2, 1, Np, 7], the layout of
+    ``hislam2/pgo_buffer.py:global_relative_posesim3_constraints``.
+    """
+    p = make_ba_problem(name, seed=seed, device="cpu")
+    g = torch.Generator().manual_seed(seed + 2000)
+    K, t0, t1 = p["poses"].shape[0], p["t0"], p["t1"]
+    s = torch.exp(scale_sigma * torch.randn(K, 1, generator=g, dtype=torch.float64)).float()
+    poses = torch.cat([p["poses"], s], 1)
+    Np = 2 * K if num_factors is None else num_factors
+    iip = torch.randint(0, t1, (Np,), generator=g)
+    jjp = torch.randint(max(t0, 1), t1, (Np,), generator=g) if t1 > max(t0, 1) else torch.zeros(Np, dtype=torch.long)
+    Ji = torch.randn(Np, 7, 7, generator=g, dtype=torch.float64)
+    Jj = torch.randn(Np, 7, 7, generator=g, dtype=torch.float64)
+    lo, hi = info_range
+    W = torch.diag_embed(10.0 ** (lo + (hi - lo) * torch.rand(Np, 7, generator=g, dtype=torch.float64)))
+    r = 0.01 * torch.randn(Np, 7, 1, generator=g, dtype=torch.float64)
+    pw = 1e-3
+    wJiT = pw * Ji.transpose(1, 2) @ W
+    wJjT = pw * Jj.transpose(1, 2) @ W
+    Hsp = torch.stack([wJiT @ Ji, wJiT @ Jj, wJjT @ Ji, wJjT @ Jj])[:, None].float()
+    vsp = (-torch.stack([wJiT @ r, wJjT @ r]).squeeze(-1))[:, None].float()
+    out = dict(p)
+    out.update(poses=poses, Hsp=Hsp, vsp=vsp, iip=iip, jjp=jjp)
+    out = {k: (v.to(device) if isinstance(v, torch.Tensor) else v) for k, v in out.items()}
+    out["Hsp"], out["vsp"] = out["Hsp"].contiguous(), out["vsp"].contiguous()
+    return out

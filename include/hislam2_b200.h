@@ -129,6 +129,31 @@ int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num_disps, int
            int iterations, float lm, float ep, int motion_only, float* dx, float* dz, int64_t dz_rows,
            int32_t* info, void* workspace, size_t workspace_bytes, hs2_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * pgba  (reference: src/droid.cpp:171-196, src/droid_kernels.cu:1940-2044)
+ *   ONE damped Gauss-Newton step over the Sim3 poses [t0,t1) and the disparity maps
+ *   of every frame in unique(cat(arange(t0,t1), ii)).  poses [num_poses,8] f32
+ *   (t, q xyzw, s) are only read: dx [t1-t0,7] f32 (tangent [tau, phi, sigma]) is
+ *   returned for the caller's Sim3 retraction; disps [num_disps,ht,wd] is updated
+ *   IN PLACE by dz.  The relative-pose factors: Hsp [4,num_factors,7,7] f32 (blocks
+ *   at (iip,iip), (iip,jjp), (jjp,iip), (jjp,jjp)), vsp [2,num_factors,7] f32 (at iip,
+ *   jjp), iip/jjp [num_factors] int64 < t1; keys below t0 are dropped as in the
+ *   reference.  intrinsics, targets, weights, eta, ii, jj as for hs2_ba.
+ *   dz [M,ht*wd] f32 with dz_rows >= min(num_poses, num_disps, t1-t0+num_edges).
+ *   info: int32[4] on the device: [0] HS2_DEV_* bits (HS2_DEV_BAD_INDEX also for
+ *   iip/jjp >= t1), [1] M, [2] 1 when the factorisation failed (dx = 0, as in the
+ *   reference).  When info[0] != 0 disps is unchanged.
+ *   workspace: hs2_pgba_workspace_size() bytes, 256-byte aligned.
+ */
+int hs2_pgba_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd, int64_t num_edges,
+                            int t0, int t1, size_t* bytes);
+int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int64_t num_disps, int ht, int wd,
+             const float* intrinsics, const float* targets, const float* weights, const float* eta,
+             int64_t eta_rows, const float* Hsp, const float* vsp, const int64_t* iip, const int64_t* jjp,
+             int64_t num_factors, const int64_t* ii, const int64_t* jj, int64_t num_edges, int t0, int t1,
+             float lm, float ep, float* dx, float* dz, int64_t dz_rows, int32_t* info, void* workspace,
+             size_t workspace_bytes, hs2_stream_t stream);
+
 /* ba without allocation.  No counterpart in the reference: this entry point is for
  * callers that cannot allocate device memory when they run a BA step (a stream
  * being captured into a CUDA graph, a process with a GPU memory budget fixed at

@@ -15,7 +15,7 @@ Pinning status (how far the oracle itself is checked against the reference):
     reference's own CUDA sources (``src/correlation_kernels.cu``,
     ``src/altcorr_kernel.cu``) compiled unmodified into ``oracle/_ref`` and run on
     a GPU (golden fixtures under ``tests/golden`` plus the live GPU tests).
-  * ba, frame_distance, iproj, covis_distance, depth_filter: parity unpinned.  ``src/droid_kernels.cu`` cannot be
+  * ba, pgba, frame_distance, iproj, covis_distance, depth_filter: parity unpinned.  ``src/droid_kernels.cu`` cannot be
     built here (it includes Eigen, which is absent), the reference has no tests
     or golden vectors, and its Python path needs lietorch/torch_scatter (absent).
     These oracle functions are instead checked by independent mathematical
@@ -23,4 +23,4 @@ Pinning status (how far the oracle itself is checked against the reference):
     Schur complement against a direct joint solve).
 """
 
-from . import se3, ba, corr, frame_distance, geometry  # noqa: F401
+from . import se3, ba, corr, frame_distance, geometry, pgba  # noqa: F401

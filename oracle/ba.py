@@ -173,10 +173,11 @@ def assemble_pose_system(Hs, vs, ii, jj, t0, P):
     ``ba_cuda`` :1882-1889, ``SparseBlock`` :1598-1638: negative keys are dropped,
     duplicates are summed.
     """
+    D = Hs.shape[-1]
     ii = np.asarray(ii, dtype=np.int64) - t0
     jj = np.asarray(jj, dtype=np.int64) - t0
-    A = np.zeros((P, 6, P, 6))
-    b = np.zeros((P, 6))
+    A = np.zeros((P, D, P, D))
+    b = np.zeros((P, D))
     rows = [ii, ii, jj, jj]
     cols = [ii, jj, ii, jj]
     for blk in range(4):
@@ -185,7 +186,7 @@ def assemble_pose_system(Hs, vs, ii, jj, t0, P):
     for blk, keys_ in enumerate([ii, jj]):
         m = keys_ >= 0
         np.add.at(b, keys_[m], vs[blk][m])
-    return A.reshape(6 * P, 6 * P), b.reshape(-1)
+    return A.reshape(D * P, D * P), b.reshape(-1)
 
 
 def schur_rows(jj_exp, kk_exp, t0, t1):
@@ -231,40 +232,41 @@ def schur_complement(E, Q, w, jj_exp, kk_exp, t0, t1):
     jj_exp[n]-t0, negatives dropped (``Ev6x1_kernel`` :1525-1560, :1775).
     """
     P = t1 - t0
-    HW = E.shape[-1]
-    S = np.zeros((P, 6, P, 6))
-    bS = np.zeros((P, 6))
+    D, HW = E.shape[1], E.shape[-1]
+    S = np.zeros((P, D, P, D))
+    bS = np.zeros((P, D))
     jj_exp = np.asarray(jj_exp, dtype=np.int64)
     kk_exp = np.asarray(kk_exp, dtype=np.int64)
     for k, rows in schur_rows(jj_exp, kk_exp, t0, t1).items():
         F = E[rows].reshape(-1, HW)
         Sk = (F * Q[k]) @ F.T
         pr = jj_exp[rows] - t0
-        Sk = Sk.reshape(len(rows), 6, len(rows), 6)
+        Sk = Sk.reshape(len(rows), D, len(rows), D)
         for a in range(len(rows)):
             np.add.at(S, (pr[a], slice(None), pr), np.swapaxes(Sk[a], 0, 1))
     v = np.einsum("ndp,np->nd", E, (Q * w)[kk_exp])
     keys_ = jj_exp - t0
     m = keys_ >= 0
     np.add.at(bS, keys_[m], v[m])
-    return S.reshape(6 * P, 6 * P), bS.reshape(-1)
+    return S.reshape(D * P, D * P), bS.reshape(-1)
 
 
-def solve(A, b, lm, ep):
-    """``SparseBlock::solve`` (:1660-1680): diag += ep + lm*diag, LLT, zeros on failure."""
+def solve(A, b, lm, ep, D=6):
+    """``SparseBlock::solve`` (:1660-1680): diag += ep + lm*diag, LLT, zeros on failure.
+    Only the lower triangle of A is read, as ``SimplicialLLT`` does."""
     n = A.shape[0]
     L = np.array(A, dtype=np.float64, copy=True)
     if n == 0:
-        return np.zeros((0, 6)), True
+        return np.zeros((0, D)), True
     di = np.arange(n)
     L[di, di] += ep + lm * L[di, di]
     try:
         C = np.linalg.cholesky(L)
     except np.linalg.LinAlgError:
-        return np.zeros((n // 6, 6)), False
+        return np.zeros((n // D, D)), False
     y = np.linalg.solve(C, b)
     x = np.linalg.solve(C.T, y)
-    return x.reshape(-1, 6), True
+    return x.reshape(-1, D), True
 
 
 def back_substitute(E, Q, w, dx, ii_exp, jj_exp, kx, t0, P, skip_t0=True):

@@ -105,3 +105,30 @@ def proj(X, intr):
     fx, fy, cx, cy = intr
     with np.errstate(divide="ignore", invalid="ignore"):
         return fx * (X[..., 0] / X[..., 2]) + cx, fy * (X[..., 1] / X[..., 2]) + cy
+
+
+# Sim3 poses are ``[tx, ty, tz, qx, qy, qz, qw, s]`` (``droid_kernels.cu:648-663``).
+
+def act_sim3(t, q, s, X):
+    """Homogeneous point [X, Y, Z, d] under (t, q, s): (s R X + d t, d)
+    (``droid_kernels.cu:96-102`` actSim3)."""
+    Y = s[..., None] * act_so3(q, X[..., :3]) + X[..., 3:4] * t
+    return np.concatenate([Y, X[..., 3:4]], axis=-1)
+
+
+def adj_sim3(t, q, s, X):
+    """The map of ``adjSim3`` (``droid_kernels.cu:122-145``) used for Ji = -adj(Gij, Jj):
+    [s R^T a, s (R^T b + R^T (a x t)) + c t, c] for X = [a, b, c] (3 + 3 + 1)."""
+    Y = adj_se3(t, q, X[..., :6])
+    c = X[..., 6:7]
+    s_ = s[..., None]
+    return np.concatenate([s_ * Y[..., :3], s_ * Y[..., 3:6] + c * t, c], axis=-1)
+
+
+def rel_sim3(ti, qi, si, tj, qj, sj):
+    """Gij = Gj * Gi^-1 for Sim3: qij as relSE3, sij = sj / si, tij = tj - sij R(qij) ti
+    (``droid_kernels.cu:162-177`` relSim3)."""
+    _, qij = rel_se3(ti, qi, tj, qj)
+    sij = sj / si
+    tij = tj - sij[..., None] * act_so3(qij, ti)
+    return tij, qij, sij

@@ -92,10 +92,15 @@ def test_ops_check_contiguity_then_device():
         droid_backends.frame_distance(p, d, torch.zeros(4), i, i, 0.3)
 
 
-def test_out_of_path_ops_raise():
-    for name in ("pgba",):
-        with pytest.raises(NotImplementedError, match=name):
-            getattr(droid_backends, name)()
+def test_pgba_checks_inputs_on_cpu():
+    p, d, i = torch.zeros(4, 8), torch.ones(4, 3, 3), torch.zeros(2, dtype=torch.long)
+    args = (torch.zeros(4), torch.zeros(2, 2, 3, 3), torch.zeros(2, 2, 3, 3), torch.ones(4, 3, 3),
+            torch.zeros(4, 1, 1, 7, 7), torch.zeros(2, 1, 1, 7), i, i, i[:1], i[:1], 1, 4, 1e-4, 0.1)
+    with pytest.raises(RuntimeError, match="poses must be contiguous"):
+        droid_backends.pgba(torch.zeros(8, 4).t(), d, *args)
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        droid_backends.pgba(p, d, *args)
+    assert backends.pgba is droid_backends.pgba
 
 
 def test_geometry_ops_check_inputs_on_cpu():
