@@ -2497,7 +2497,7 @@ constexpr int kPgH = 35;          // upper triangle of Hjj (28), then vj (7)
 constexpr int kPgThreads = 256;
 constexpr int kPgPPT = 4;
 constexpr int kPgChunk = kPgThreads * kPgPPT;
-constexpr int kPgSplit = 8;       // CTAs per depth frame in the Gram
+constexpr int kPgSplit = 16;      // CTAs per depth frame in the Gram
 
 __host__ __device__ __forceinline__ int64_t pg_order(int P) { return 7 * (int64_t)P + ((7 * (int64_t)P) & 1); }
 
@@ -2757,66 +2757,80 @@ __global__ void pg_pad_kernel(double* __restrict__ A, int64_t n, int64_t npad) {
   if (threadIdx.x == 0 && blockIdx.x == 0 && npad > n) A[n * npad + n] = 1.0;
 }
 
-// Gram of a frame's Schur rows (stored at rptr[s] + a, a < nr, in srow order): 32 x 32 output tiles of the (7 R) x (7 R) matrix
-// G_xy = sum_p E_x Q E_y, lower tiles only, tiles spread over gridDim.y CTAs.  Each
-// unordered pair {x, y} of the full Gram is subtracted once at the lower-triangle
-// position of the system it maps to (twice onto a diagonal entry hit by both orders).
-__global__ void __launch_bounds__(256)
+// Gram of a frame's Schur rows (stored at rptr[s] + a, a < nr, in srow order): 32 x 32 output tiles
+// of the (7 R) x (7 R) matrix G_xy = sum_p E_x Q E_y, lower tiles only, spread over
+// gridDim.y CTAs of 64 threads.  Pixels are staged 32 at a time k-major in shared memory
+// (thread (rh, pc) loads pixel column pc of rows rh, rh + 2, ..); each thread keeps a
+// 4 x 4 block of outputs and reads its operands as float4.  Each unordered pair {x, y}
+// of the full Gram is subtracted once at the lower-triangle position of the system it
+// maps to (twice onto a diagonal entry hit by both orders).
+constexpr int kPgGT = 32;   // Gram tile (outputs per side)
+constexpr int kPgGK = 32;   // pixels per stage
+constexpr int kPgGThreads = 64;
+
+__global__ void __launch_bounds__(kPgGThreads)
 pg_schur_kernel(int HW, int64_t npad, BaPtrs w, const float* __restrict__ erows, const float* __restrict__ qbuf,
                 double* __restrict__ A, const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int r0 = w.sptr[s], nr = w.sptr[s + 1] - r0;
-  const size_t rbase = (size_t)w.rptr[s];   // storage position of the frame's first Schur row
-  const int m = kPgD * nr, nt = (m + 31) / 32, T = nt * (nt + 1) / 2;
-  const size_t HWs = (size_t)row_stride(HW);
-  __shared__ float Xs[32][33], Ys[32][33];
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int64_t rbase = w.rptr[s];   // storage position of the frame's first Schur row
+  const int m = kPgD * nr, nt = (m + kPgGT - 1) / kPgGT, T = nt * (nt + 1) / 2;
+  const int64_t HWs = row_stride(HW);
+  __shared__ __align__(16) float Xs[kPgGK][kPgGT + 4];
+  __shared__ __align__(16) float Ys[kPgGK][kPgGT + 4];
+  const int tid = threadIdx.x, ty = tid >> 3, tx = tid & 7;
+  const int pc = tid & 31, rh = tid >> 5;
   const float* Q = qbuf + (int64_t)s * HW;
   for (int t = blockIdx.y; t < T; t += gridDim.y) {
     int ti = 0;
     while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
     const int tj = t - ti * (ti + 1) / 2;
-    float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-    for (int p0 = 0; p0 < HW; p0 += 32) {
+    // plane offsets of the 16 rows this thread stages for each side (-1: past the last row)
+    int64_t ox[16], oy[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int x = kPgGT * ti + rh + 2 * q, y = kPgGT * tj + rh + 2 * q;
+      ox[q] = x < m ? ((rbase + x / kPgD) * kPgD + x % kPgD) * HWs : -1;
+      oy[q] = y < m ? ((rbase + y / kPgD) * kPgD + y % kPgD) * HWs : -1;
+    }
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    for (int p0 = 0; p0 < HW; p0 += kPgGK) {
+      const int p = p0 + pc;
+      const bool ok = p < HW;
+      const float qv = ok ? Q[p] : 0.f;
       __syncthreads();
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int idx = tid + q * 256, rl = idx >> 5, pc = idx & 31, p = p0 + pc;
-        const int x = 32 * ti + rl, y = 32 * tj + rl;
-        float vx = 0.f, vy = 0.f;
-        if (p < HW && x < m) {
-          const size_t row = rbase + x / kPgD;
-          vx = erows[(row * kPgD + x % kPgD) * HWs + p] * Q[p];
-        }
-        if (p < HW && y < m) {
-          const size_t row = rbase + y / kPgD;
-          vy = erows[(row * kPgD + y % kPgD) * HWs + p];
-        }
-        Xs[rl][pc] = vx;
-        Ys[rl][pc] = vy;
+      for (int q = 0; q < 16; ++q) {
+        Xs[pc][rh + 2 * q] = (ok && ox[q] >= 0) ? erows[ox[q] + p] * qv : 0.f;
+        Ys[pc][rh + 2 * q] = (ok && oy[q] >= 0) ? erows[oy[q] + p] : 0.f;
       }
       __syncthreads();
 #pragma unroll 8
-      for (int k = 0; k < 32; ++k) {
-        const float a0 = Xs[ty][k], a1 = Xs[ty + 16][k], b0 = Ys[tx][k], b1 = Ys[tx + 16][k];
-        acc[0][0] += a0 * b0;
-        acc[0][1] += a0 * b1;
-        acc[1][0] += a1 * b0;
-        acc[1][1] += a1 * b1;
+      for (int k = 0; k < kPgGK; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(&Xs[k][4 * ty]);
+        const float4 b = *reinterpret_cast<const float4*>(&Ys[k][4 * tx]);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
       }
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int x = 32 * ti + ty + 16 * u, y = 32 * tj + tx + 16 * v;
+      for (int j = 0; j < 4; ++j) {
+        const int x = kPgGT * ti + 4 * ty + i, y = kPgGT * tj + 4 * tx + j;
         if (x >= m || y >= m || (ti == tj && x < y)) continue;
-        const double g = (double)acc[u][v];
-        const int ax = x / kPgD, dx = x % kPgD, ay = y / kPgD, dy = y % kPgD;
-        const int64_t pa = w.spose[r0 + ax], pb = w.spose[r0 + ay];
-        const int64_t gx = 7 * pa + dx, gy = 7 * pb + dy;
+        const double g = (double)acc[i][j];
+        const int64_t pa = w.spose[r0 + x / kPgD], pb = w.spose[r0 + y / kPgD];
+        const int64_t gx = 7 * pa + x % kPgD, gy = 7 * pb + y % kPgD;
         if (x == y) atomicAdd(&A[gx * npad + gy], -g);
         else if (gx > gy) atomicAdd(&A[gx * npad + gy], -g);
         else if (gy > gx) atomicAdd(&A[gy * npad + gx], -g);
@@ -3024,7 +3038,7 @@ extern "C" int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int
   }
   if (P > 0 && S > 0) {
     HS2_PROF("pg_schur", s);
-    pg_schur_kernel<<<dim3((unsigned)S, kPgSplit), 256, 0, s>>>(p.HW, npad, w, erows, qbuf, w.A, info);
+    pg_schur_kernel<<<dim3((unsigned)S, kPgSplit), kPgGThreads, 0, s>>>(p.HW, npad, w, erows, qbuf, w.A, info);
     HS2_LAUNCH_CHECK("pg_schur_kernel");
     pg_schur_rhs_kernel<<<(unsigned)S, 256, 0, s>>>(p.HW, w, erows, qbuf, wbuf, w.b, info);
     HS2_LAUNCH_CHECK("pg_schur_rhs_kernel");
