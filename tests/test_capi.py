@@ -56,6 +56,19 @@ def test_workspace_size_validation():
         8, 8, 48, 64, 24, 2, 8, False)
 
 
+def test_pgba_workspace_size_validation():
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.hs2_pgba_workspace_size(300, 300, 43, 77, 6000, 10, 300, ctypes.byref(n)) == _lib.HS2_OK
+    # holds the 7-plane E rows and the FP64 system of order 7 * 290 (even, no pad)
+    assert n.value > 7 * 6290 * 3328 * 4 + 8 * 2030 * 2030
+    m = ctypes.c_size_t(0)
+    assert lib.hs2_pgba_workspace_size(300, 300, 43, 77, 6000, 11, 300, ctypes.byref(m)) == _lib.HS2_OK
+    assert m.value >= 8 * 2024 * 2024   # order 7 * 289 = 2023 padded to 2024
+    assert lib.hs2_pgba_workspace_size(300, 300, 43, 77, 6000, 10, 301, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+    assert b"t1" in lib.hs2_last_error()
+
+
 def test_corr_validation_before_any_launch():
     lib = _lib.load()
     rc = lib.hs2_corr_index_forward(None, _lib.HS2_F32, 1, 4, 4, 4, 4, None, -1, None, None)
