@@ -67,6 +67,20 @@ def test_pgba_matches_oracle_frontend_window(cuda):
     _check(p, dx, dz, disps)
 
 
+@pytest.mark.parametrize("t0", [0, 8], ids=["whole_buffer", "empty_window"])
+def test_pgba_window_edges(cuda, t0):
+    # t0 = 0: the reference's back-substitution skips pose 0 (ix <= 0); t0 = t1: no pose
+    # is optimised, dx is empty and dz = Q w
+    p, g = _problem(cuda, t0=t0)
+    dx, dz, disps = _run(g)
+    assert dx.shape == (p["t1"] - t0, 7)
+    if t0 == p["t1"]:
+        ref = _oracle(p)
+        np.testing.assert_allclose(dz.cpu().numpy(), ref.dz, rtol=1e-4, atol=1e-4 * np.abs(ref.dz).max())
+    else:
+        _check(p, dx, dz, disps)
+
+
 def test_pgba_without_factors(cuda):
     p, g = _problem(cuda, num_factors=0)
     dx, dz, disps = _run(g)
