@@ -88,7 +88,8 @@ static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) 
   L.L11 = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB * kNB);
   L.dinv = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB);
   L.ychol = take(sizeof(double) * (size_t)(n + 1));
-  L.ctl = take(sizeof(unsigned) * (4 + 2 * (size_t)((n + kNB - 1) / kNB)));   // barrier words, ready flags, slice counters
+  L.ctl = take(sizeof(unsigned) * (4 + 3 * (size_t)((n + kNB - 1) / kNB) +
+                                    (size_t)((n + kNB - 1) / kNB) * ((n + kNB - 1) / kNB)));   // see CholBuf
   L.total = o;
   return L;
 }
@@ -1483,7 +1484,9 @@ struct CholBuf {
   double* dinv;     // [nbk][64] reciprocals of their diagonals
   double* y;        // [n] forward-substituted right-hand side
   unsigned* ctl;    // [0] barrier count, [1] barrier generation, [2] failed, [4 + c] ready flags,
-                    // [4 + nbk + R] phase-A slices done on block row R
+                    // [4 + nbk + R] phase-A slices done on block row R,
+                    // [4 + 2 nbk + R] panels whose L of block row R is written,
+                    // [4 + 3 nbk + R nbk + C] trailing (phase-B) updates applied to tile (R, C)
 };
 
 __device__ __forceinline__ double2 ldcg2(const double* p) {
@@ -1562,6 +1565,35 @@ __device__ bool chol_wait_slices(const unsigned* slices, int kb, int t, int32_t*
   }
   __syncthreads();
   return s_bad == 0;
+}
+
+// Waits (thread 0) until *c >= target; false on timeout, or at once when another wait of
+// the launch has already timed out.
+__device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target, int32_t* info) {
+  unsigned spins = 0;
+  while (ld_acquire_gpu(c) < target) {
+    if ((++spins & 255u) == 0 && (*(volatile int32_t*)info & HS2_DEV_TIMEOUT)) return false;
+    if (spins > kBarrierSpins) {
+      atomicOr(info, HS2_DEV_TIMEOUT);
+      return false;
+    }
+    if (spins > 64) __nanosleep(32);
+  }
+  return true;
+}
+
+// A trailing-update task on tile (R, C) with panel kb: waits until panel kb has written
+// the L blocks of rows R and C and the tile holds the phase-B updates of panels < kb
+// (tcnt >= tdone).  CTA-wide result.
+__device__ bool chol_wait_tile(const unsigned* lcnt, const unsigned* tcnt, int nbk, int kb, int R, int C,
+                               unsigned tdone, int32_t* info) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    s_ok = wait_count(lcnt + R, kb + 1, info) && wait_count(lcnt + C, kb + 1, info) &&
+           wait_count(tcnt + (int64_t)R * nbk + C, tdone, info);
+  __syncthreads();
+  return s_ok != 0;
 }
 
 // Waits (thread 0) until the ready flag is set; false on timeout.
@@ -1997,27 +2029,36 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
   }
   if (!grid_barrier(cb.ctl, G, info)) return;
 
-  for (int t = blockIdx.x; t < nbk; t += G)
-    if (!chol_panel(n, 0, t, A, bvec, cb, csm)) break;
-  if (!grid_barrier(cb.ctl, G, info)) return;
-  bool failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
+  // Dataflow instead of a grid barrier per panel: every task waits (acquire) only for the
+  // tasks that write its inputs and counts itself (release) when done.  A task of stage
+  // A(kb) / B(kb) depends only on tasks of earlier stages and every CTA runs its tasks in
+  // stage order, so with all CTAs resident (cooperative launch) no wait can cycle.  A
+  // failed factorisation does not stop the schedule (results are discarded at the end).
+  unsigned* slices = cb.ctl + kCtlFlags + nbk;
+  unsigned* lcnt = cb.ctl + kCtlFlags + 2 * nbk;
+  unsigned* tcnt = cb.ctl + kCtlFlags + 3 * nbk;
+  for (int t = blockIdx.x; t < nbk; t += G) {
+    chol_panel(n, 0, t, A, bvec, cb, csm);
+    __syncthreads();
+    if (threadIdx.x == 0 && t > 0) red_release_add_gpu(lcnt + t, 1u);
+  }
 
-  for (int kb = 0; kb + 1 < nbk && !failed; ++kb) {
+  for (int kb = 0; kb + 1 < nbk; ++kb) {
     const int o = kb * kNB;
     const int rest = nbk - kb - 1;
     // A: column block kb+1, 16-row slices of the tiles below panel kb; each slice counts
-    // itself on its block row (release), which the panel tasks of phase B wait for instead
-    // of a grid barrier
-    unsigned* slices = cb.ctl + kCtlFlags + nbk;
+    // itself on its block row, which the panel tasks of phase B wait for
     for (int t = blockIdx.x; t < rest * 4; t += G) {
       const int I = t >> 2, q = t & 3;
+      if (!chol_wait_tile(lcnt, tcnt, nbk, kb, kb + 1 + I, kb + 1, (unsigned)kb, info)) return;
       chol_update_tile<1>(n, A, o, o + kNB + I * kNB + 16 * q, o + kNB, I == 0, csm);
       __syncthreads();
       if (threadIdx.x == 0) red_release_add_gpu(slices + kb + 1 + I, 1u);
     }
     // B: panel kb+1 (tasks 0..rest-1) || tiles (I, J), 1 <= J <= I < rest, of update kb.
     // The panel tasks sit on CTAs of their own (they are the longer tasks); the tiles go
-    // round-robin over the remaining CTAs.
+    // round-robin over the remaining CTAs.  A panel task counts the L block it writes on
+    // its block row; a tile counts the update it applied.
     const int ntiles = rest * (rest - 1) / 2;
     const bool split = (int)G > rest;
     const int tfirst = split ? ((int)blockIdx.x < rest ? ntiles : (int)blockIdx.x - rest) : (int)blockIdx.x;
@@ -2025,11 +2066,15 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
     if (split && (int)blockIdx.x < rest) {
       if (!chol_wait_slices(slices, kb, blockIdx.x, info)) return;
       chol_panel(n, kb + 1, blockIdx.x, A, bvec, cb, csm);
+      __syncthreads();
+      if (threadIdx.x == 0 && blockIdx.x > 0) red_release_add_gpu(lcnt + kb + 1 + blockIdx.x, 1u);
     }
     for (int t = tfirst; t < (split ? ntiles : rest + ntiles); t += tstep) {
       if (!split && t < rest) {
         if (!chol_wait_slices(slices, kb, t, info)) return;
         chol_panel(n, kb + 1, t, A, bvec, cb, csm);
+        __syncthreads();
+        if (threadIdx.x == 0 && t > 0) red_release_add_gpu(lcnt + kb + 1 + t, 1u);
         continue;
       }
       int I = 0, tt = split ? t : t - rest;
@@ -2039,11 +2084,14 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
       }
       const int J = tt + 1;
       ++I;
+      if (!chol_wait_tile(lcnt, tcnt, nbk, kb, kb + 1 + I, kb + 1 + J, (unsigned)kb, info)) return;
       chol_update_tile<4>(n, A, o, o + kNB + I * kNB, o + kNB + J * kNB, I == J, csm);
+      __syncthreads();
+      if (threadIdx.x == 0) red_release_add_gpu(tcnt + (int64_t)(kb + 1 + I) * nbk + kb + 1 + J, 1u);
     }
-    if (!grid_barrier(cb.ctl, G, info)) return;
-    failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
   }
+  if (!grid_barrier(cb.ctl, G, info)) return;
+  const bool failed = *(volatile unsigned*)(cb.ctl + 2) != 0;
 
   if (!failed) {
     chol_backward(n, nbk, A, cb, w.x, dx_out, info, csm);
@@ -2196,7 +2244,7 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   }
   const int work = std::max(std::max(nbk, (nbk - 1) * nbk / 2), (n + kCholThreads - 1) / kCholThreads);
   int G = std::max(1, std::min(grid_cap[dev], work));
-  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + 2 * nbk) * sizeof(unsigned), s));
+  HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + 3 * (size_t)nbk + (size_t)nbk * nbk) * sizeof(unsigned), s));
   void* args[] = {&n, &lm, &ep, &w, &cb, &dx, &info};
   HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_cholesky_kernel, dim3(G), dim3(kCholThreads), args, smem, s));
   HS2_LAUNCH_CHECK("ba_cholesky_kernel");
@@ -2935,7 +2983,7 @@ static PgLayout pg_layout(int64_t K, int HW, int64_t E, int P) {
   L.L11 = take(sizeof(double) * (size_t)nbk * kNB * kNB);
   L.dinv = take(sizeof(double) * (size_t)nbk * kNB);
   L.ychol = take(sizeof(double) * (size_t)(n + 1));
-  L.ctl = take(sizeof(unsigned) * (4 + 2 * (size_t)nbk));
+  L.ctl = take(sizeof(unsigned) * (4 + 3 * (size_t)nbk + (size_t)nbk * nbk));
   L.total = o;
   return L;
 }
