@@ -260,6 +260,7 @@ def run_ours(args, world, rank, local):
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     corr = corr_lookup(args, dev, world, peaks)
+    pg = pgba_leg(args, dev, world, rank)
 
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = json.load(open(traffic_path)) if os.path.exists(traffic_path) else {}
@@ -277,7 +278,7 @@ def run_ours(args, world, rank, local):
                 "config": dict(CONFIG, parallelism="replicas: one independent window per rank" if world > 1 else
                                "single GPU"),
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "corr_lookup": corr, "clocks": clk,
+                "corr_lookup": corr, "pgba": pg, "clocks": clk,
                 "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
                 "simt_peaks_tflops": {"fp32": round(simt[0], 2), "fp64": round(simt[1], 2)}}
         print(json.dumps(line), flush=True)
@@ -329,6 +330,43 @@ def corr_lookup(args, dev, world, peaks):
             "config": "258 edges (frontend window), 43x77, 4 levels, radius 4, fp16 volumes",
             "roofline": {"bound": "hbm", "achieved": round(gbs / world, 2), "peak": peaks["hbm_gbs"],
                          "unit": "GB/s", "frac": round(gbs / world / peaks["hbm_gbs"], 4)}}
+
+
+def pgba_leg(args, dev, world, rank):
+    """One Sim3 pose-graph BA step (droid_backends.pgba) on the same 300-keyframe /
+    6000-edge window with Sim3 poses and 600 relative-pose factors, device-timed."""
+    import droid_backends
+    from hislam2_b200 import _lib, replicas, synth
+
+    g = synth.make_pgba_problem(WORKLOAD, seed=replicas.window_seed(rank), device=dev, num_factors=600)
+    init = g["disps"].clone()
+    disps = init.clone()
+
+    def step():
+        disps.copy_(init)
+        droid_backends.pgba(g["poses"], disps, g["intrinsics"], g["targets"], g["weights"], g["eta"], g["Hsp"],
+                            g["vsp"], g["ii"], g["jj"], g["iip"], g["jjp"], g["t0"], g["t1"], g["lm"], g["ep"])
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    _lib.profile_report(reset=True)
+    _lib.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    _lib.profile_enable(False)
+    prof = _lib.profile_report(reset=True)
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.steps
+    del g, init, disps
+    torch.cuda.empty_cache()
+    return {"value": round(world * 1e3 / ms, 2), "unit": "pgba steps/s", "ms_per_step": round(ms, 4),
+            "config": "backend300 window with Sim3 poses, 600 relative-pose factors, one GN step",
+            "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())}}
 
 
 # ------------------------------------------------------------ CPU oracle legs
