@@ -44,9 +44,9 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
 
 
-def _raise_device_errors(bits, op):
+def _raise_device_errors(bits, op, indices="ii/jj outside the buffers or >= t1"):
     if bits & _lib.HS2_DEV_BAD_INDEX:
-        raise RuntimeError("%s: an edge index is out of range (ii/jj outside the buffers or >= t1)" % op)
+        raise RuntimeError("%s: an edge index is out of range (%s)" % (op, indices))
     if bits & _lib.HS2_DEV_BAD_ETA:
         raise RuntimeError("%s: eta must have M or 1 rows (M = number of distinct depth frames)" % op)
     if bits & _lib.HS2_DEV_TIMEOUT:
@@ -198,7 +198,7 @@ def pgba(poses, disps, intrinsics, targets, weights, eta, Hsp, vsp, ii, jj, iip,
         eta.numel() // (ht * wd), _ptr(Hsp), _ptr(vsp), _ptr(iip), _ptr(jjp), Np, _ptr(ii), _ptr(jj), E, t0, t1,
         float(lm), float(ep), _ptr(dx), _ptr(dz), S, _ptr(info), _ptr(ws), ws_bytes, _stream(dev)), "pgba")
     h = info.cpu()
-    _raise_device_errors(int(h[0]), "pgba")
+    _raise_device_errors(int(h[0]), "pgba", "ii/jj outside the buffers or >= t1, or iip/jjp >= t1")
     return [dx, dz[:int(h[1])]]
 
 
