@@ -24,6 +24,9 @@
 //
 // Only the (tiny) key generation is serial; everything else is sized by the
 // static problem dimensions, so a whole call is graph-capturable.
+//
+// The end of the file holds pgba (Sim3 poses, D = 7, one step with relative-pose
+// factors), which reuses the keys, the E-row layout and the Cholesky.
 #include <algorithm>
 #include <atomic>
 #include <cstring>
