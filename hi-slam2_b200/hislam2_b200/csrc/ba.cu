@@ -2234,19 +2234,21 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   HS2_PROF("ba_cholesky", s);
   const int nbk = (n + kNB - 1) / kNB;
   const size_t smem = sizeof(double) * (128 * kPLD + 128 + 64 + 72 + 2);   // panel (tile, backward need less)
-  static int grid_cap[64] = {0};
+  static DeviceOnce once;
+  static std::atomic<int> grid_cap[kMaxDevices];
   int dev = 0;
   HS2_CUDA(cudaGetDevice(&dev));
-  if (dev >= 64) dev = 63;
-  if (grid_cap[dev] == 0) {
+  int rc = once.run(dev, [&]() -> int {
     int sms = 0, occ = 0;
     HS2_CUDA(cudaFuncSetAttribute(ba_cholesky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HS2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     HS2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ba_cholesky_kernel, kCholThreads, smem));
-    grid_cap[dev] = std::max(1, std::min(occ, 1) * sms);
-  }
+    grid_cap[dev].store(std::max(1, std::min(occ, 1) * sms), std::memory_order_relaxed);
+    return HS2_OK;
+  });
+  if (rc) return rc;
   const int work = std::max(std::max(nbk, (nbk - 1) * nbk / 2), (n + kCholThreads - 1) / kCholThreads);
-  int G = std::max(1, std::min(grid_cap[dev], work));
+  int G = std::max(1, std::min(grid_cap[dev].load(std::memory_order_relaxed), work));
   HS2_CUDA(cudaMemsetAsync(cb.ctl, 0, (kCtlFlags + 3 * (size_t)nbk + (size_t)nbk * nbk) * sizeof(unsigned), s));
   void* args[] = {&n, &lm, &ep, &w, &cb, &dx, &info};
   HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_cholesky_kernel, dim3(G), dim3(kCholThreads), args, smem, s));
@@ -2316,13 +2318,14 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
   const int path = g_schur_path.load();
   const bool fused = !p.motion_only && path == 2;
   if (fused && S > 0) {
-    static bool attr_set[64] = {false};
+    static DeviceOnce once;
     int dev = 0;
     HS2_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !attr_set[dev]) {
+    int rc = once.run(dev, [&]() -> int {
       HS2_CUDA(cudaFuncSetAttribute(ba_frame_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
-      attr_set[dev] = true;
-    }
+      return HS2_OK;
+    });
+    if (rc) return rc;
     dim3 grid((unsigned)S, l.f_split);
     HS2_PROF("ba_frame", s);
     ba_frame_kernel<<<grid, kFThreads, kFSmem, s>>>(disps, p.HW, p.wd, intrinsics, targets, weights, eta, eta_rows,
@@ -2346,15 +2349,16 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
     HS2_PROF("ba_schur", s);
     const bool simt_only = path != 0;
     if (!simt_only) {
-      static bool attr_set[64] = {false};
+      static DeviceOnce once;
       int dev = 0;
       HS2_CUDA(cudaGetDevice(&dev));
-      if (dev < 64 && !attr_set[dev]) {
+      int rc = once.run(dev, [&]() -> int {
         HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-        attr_set[dev] = true;
-      }
+        return HS2_OK;
+      });
+      if (rc) return rc;
       CUtensorMap emap;
-      int rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
+      rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
       if (rc) return rc;
       dim3 grid((unsigned)S, 1u, l.tc_split);
       ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info);

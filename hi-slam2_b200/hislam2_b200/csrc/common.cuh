@@ -11,6 +11,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
 #include <type_traits>
 
 #include "hislam2_b200.h"
@@ -42,6 +44,28 @@ void count_launch();
 // Makes the device that owns `ptr` current for this thread (a no-op when it
 // already is).  All entry points take device pointers from the caller.
 int bind_device(const void* ptr);
+
+// One-time per-device set-up (kernel attributes, occupancy queries) that any
+// host thread may trigger.  `run(dev)` executes `fn` at most once per device
+// ordinal that succeeds, under a mutex; ordinals >= kMaxDevices are refused.
+constexpr int kMaxDevices = 64;
+struct DeviceOnce {
+  std::atomic<bool> done[kMaxDevices] = {};
+  std::mutex mu;
+  template <typename F>
+  int run(int dev, F&& fn) {
+    if (dev < 0 || dev >= kMaxDevices) {
+      set_error("device ordinal %d out of range (at most %d devices)", dev, kMaxDevices);
+      return HS2_ERR_INVALID;
+    }
+    if (done[dev].load(std::memory_order_acquire)) return HS2_OK;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev].load(std::memory_order_relaxed)) return HS2_OK;
+    const int rc = fn();
+    if (rc == HS2_OK) done[dev].store(true, std::memory_order_release);
+    return rc;
+  }
+};
 
 // ----------------------------------------------------------- conversions ---
 template <typename T> __device__ __forceinline__ float to_f(T v);

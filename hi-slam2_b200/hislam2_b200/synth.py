@@ -14,7 +14,10 @@ Workloads (name: keyframes, grid, edges, window, iterations, damping):
   * ``backend300``      300 kf, 43x77, 6000 edges: all 1<=|i-j|<=2 (1194) + 2403
     random loop pairs |i-j|>2 in both directions (4806), t0=10, 8 iters,
     lm=1e-5, ep=1e-2, 5% target outliers U[-20,20] px with weight 0;
-  * ``clips2x7``        2 clips x 7 frames, 48x64, all 42 edges i!=j per clip, radius 4.
+  * ``clips2x7``        2 clips x 7 frames, 48x64, all 42 edges i!=j per clip, radius 4;
+  * ``tiny6`` / ``tiny7`` 6 / 7 kf at 12x16 (96x128 image), 3 iters: the golden-fixture
+    problems (a self-edge, a duplicate edge, a loop pair; tiny7 optimises the window
+    [1, 6) of a 7-frame buffer whose last frame is unused, with 5% outliers).
 Common: ground-truth poses = identity (+) se3 noise sigma 0.05, targets = ground-
 truth reprojection + N(0, 0.5 px), weights U[0,1] per channel, eta = 1e-3; the
 optimised poses start from the ground truth (+) se3 noise sigma 0.01.
@@ -35,6 +38,10 @@ CONFIGS = {
                        disp=(0.1, 2.0), outliers=0.05),
     "clips2x7": dict(K=7, ht=48, wd=64, img=(384, 512), t0=2, iters=2, lm=1e-4, ep=0.1, radius=4,
                      disp=(0.2, 1.0), outliers=0.0),
+    "tiny6": dict(K=6, ht=12, wd=16, img=(96, 128), t0=2, iters=3, lm=1e-4, ep=0.1, radius=3,
+                  disp=(0.2, 1.0), outliers=0.0),
+    "tiny7": dict(K=7, ht=12, wd=16, img=(96, 128), t0=1, t1=6, iters=3, lm=1e-4, ep=0.1, radius=3,
+                  disp=(0.2, 1.0), outliers=0.05),
 }
 
 
@@ -123,6 +130,14 @@ def edges_for(name, K, g):
         return e
     if name == "clips2x7":
         return [(i, j) for i in range(K) for j in range(K) if i != j]
+    if name == "tiny6":
+        # all 1<=|i-j|<=2, a loop pair, a duplicate edge and a self-edge
+        e = [(i, j) for i in range(K) for j in range(K) if i != j and abs(i - j) <= 2]
+        return e + [(0, 5), (5, 0), (3, 4), (2, 2)]
+    if name == "tiny7":
+        # window [1, 6) of a 7-frame buffer; frame 6 takes no part (edges need ii, jj < t1)
+        e = [(i, j) for i in range(6) for j in range(6) if i != j and abs(i - j) <= 2]
+        return e + [(0, 3), (5, 1)]
     raise KeyError(name)
 
 
@@ -153,7 +168,7 @@ def make_ba_problem(name="frontend_small", seed=0, device="cpu"):
         noise = -20 + 40 * torch.rand(E, ht, wd, 2, generator=g, dtype=torch.float64)
         targets = torch.where(out[..., None], targets + noise, targets)
         weights = torch.where(out[..., None], torch.zeros_like(weights), weights)
-    t0, t1 = cfg["t0"], K
+    t0, t1 = cfg["t0"], cfg.get("t1", K)
     poses = poses_gt.clone()
     pert = se3_exp(0.01 * torch.randn(K, 6, generator=g, dtype=torch.float64))
     poses[t0:t1] = pose_compose(pert[t0:t1], poses_gt[t0:t1])

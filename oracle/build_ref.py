@@ -1,16 +1,20 @@
-"""Builds ``oracle/_ref/hs2_ref_corr*.so`` from the reference's correlation sources.
+"""Builds ``oracle/_ref/hs2_ref_droid*.so``: HI-SLAM2's own ``droid_backends``
+extension, compiled unmodified from the checkout's ``src/`` for sm_100a.
 
-TEST INFRASTRUCTURE ONLY.  Compiles, unmodified and where they lie,
-``src/correlation_kernels.cu`` and ``src/altcorr_kernel.cu`` of the HI-SLAM2
-checkout (default ``/root/reference``) for sm_100a, with the binding in
-``oracle/ref_corr_binding.cpp``.  Nothing is copied into the repository; the
-output goes to ``oracle/_ref/`` (git-ignored) and is used by the GPU tests and
-the fixture generator to pin the oracle against the reference's own kernels.
+TEST INFRASTRUCTURE ONLY.  Compiles, where they lie, the reference's binding
+``src/droid.cpp`` and its kernels ``src/droid_kernels.cu`` (ba, pgba,
+frame_distance, proj_trans, covis_distance, depth_filter, iproj, bi_inter),
+``src/correlation_kernels.cu`` and ``src/altcorr_kernel.cu``.  Eigen, which
+``droid_kernels.cu`` includes (``:15-17``), is absent from the checkout (empty
+``thirdparty/eigen`` submodule) and from this image, so the include path puts
+the self-written dense stand-in ``oracle/eigen_standin/`` in its place (its
+header states what it restates and how it differs: natural instead of AMD
+ordering in the LLT).  Nothing is copied into the repository; the output goes to
+``oracle/_ref/`` (git-ignored) and is used by the GPU tests and the fixture
+generator to pin the numpy oracle against the reference's own operators.
 
-``src/droid_kernels.cu`` (ba, frame_distance) is not built: it includes Eigen,
-which is absent from the checkout (empty ``thirdparty/eigen`` submodule).
-
-Usage: ``python oracle/build_ref.py [--reference PATH]``.
+The checkout is found at ``$HISLAM2_REFERENCE``, else at the default below.
+Usage: ``python oracle/build_ref.py [--reference PATH] [-v]``.
 """
 
 import argparse
@@ -20,7 +24,13 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-NAME = "hs2_ref_corr"
+NAME = "hs2_ref_droid"
+STANDIN = os.path.join(HERE, "eigen_standin")
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_path(reference=None):
+    return reference or os.environ.get("HISLAM2_REFERENCE") or DEFAULT_REFERENCE
 
 
 def built_library():
@@ -28,9 +38,11 @@ def built_library():
     return hits[0] if hits else None
 
 
-def build(reference="/root/reference", verbose=False):
-    src = os.path.join(reference, "src")
-    sources = [os.path.join(src, "correlation_kernels.cu"), os.path.join(src, "altcorr_kernel.cu")]
+def build(reference=None, verbose=False):
+    """Returns the built library's path, or None when the checkout is absent."""
+    src = os.path.join(reference_path(reference), "src")
+    sources = [os.path.join(src, f) for f in ("droid.cpp", "droid_kernels.cu", "correlation_kernels.cu",
+                                              "altcorr_kernel.cu")]
     if not all(os.path.exists(s) for s in sources):
         return None
     os.makedirs(OUT, exist_ok=True)
@@ -38,8 +50,9 @@ def build(reference="/root/reference", verbose=False):
     os.environ.setdefault("TORCH_CUDA_ARCH_LIST", "10.0")
     cpp_extension.load(
         name=NAME,
-        sources=[os.path.join(HERE, "ref_corr_binding.cpp")] + sources,
+        sources=sources,
         build_directory=OUT,
+        extra_include_paths=[STANDIN],
         extra_cflags=["-O2"],
         extra_cuda_cflags=["-O3", "-gencode", "arch=compute_100a,code=sm_100a"],
         verbose=verbose,
@@ -65,7 +78,7 @@ def load():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     lib = build(a.reference, a.verbose)

@@ -22,7 +22,13 @@ def cuda():
 
 
 @pytest.fixture(scope="session")
-def ref_corr():
-    """The reference's own correlation kernels built in oracle/_ref (None if absent)."""
+def ref_ops():
+    """The reference's own droid_backends operators built in oracle/_ref (None if absent)."""
     from oracle import build_ref
     return build_ref.load()
+
+
+@pytest.fixture(scope="session")
+def ref_corr(ref_ops):
+    """The reference's correlation operators (the same module as ref_ops)."""
+    return ref_ops

@@ -35,12 +35,35 @@ def test_library_exports_every_declared_symbol():
     assert lib.hs2_version() == (1 << 16)
 
 
-def test_library_links_no_cuda_runtime_dynamically():
-    # cudart is linked statically so the library does not clash with PyTorch's own runtime
-    maps = open("/proc/self/maps").read()
+def elf_needed(path):
+    """DT_NEEDED entries of a 64-bit little-endian ELF shared object."""
+    import struct
+    data = open(path, "rb").read()
+    assert data[:4] == b"\x7fELF" and data[4] == 2 and data[5] == 1
+    shoff, = struct.unpack_from("<Q", data, 0x28)
+    shentsize, shnum = struct.unpack_from("<HH", data, 0x3A)
+    sections = [struct.unpack_from("<IIQQQQIIQQ", data, shoff + k * shentsize) for k in range(shnum)]
+    dyn = next(s for s in sections if s[1] == 6)          # SHT_DYNAMIC
+    strtab = sections[dyn[6]]                              # sh_link -> its string table
+    out = []
+    for off in range(dyn[4], dyn[4] + dyn[5], 16):
+        tag, val = struct.unpack_from("<qQ", data, off)
+        if tag == 0:
+            break
+        if tag == 1:                                       # DT_NEEDED
+            start = strtab[4] + val
+            out.append(data[start:data.index(b"\0", start)].decode())
+    return out
+
+
+def test_library_needs_no_shared_cuda_runtime():
+    # cudart is linked statically (nvcc's default), so the library does not depend on, or clash
+    # with, the CUDA runtime that PyTorch ships; the driver API is reached at run time instead
+    needed = elf_needed(_lib.LIB_PATH)
+    assert "libc.so.6" in needed
+    assert not any(n.startswith(("libcudart", "libtorch", "libc10")) for n in needed), needed
     _lib.load()
-    maps = open("/proc/self/maps").read()
-    assert _lib.LIB_PATH in maps
+    assert _lib.LIB_PATH in open("/proc/self/maps").read()
 
 
 def test_workspace_size_validation():
