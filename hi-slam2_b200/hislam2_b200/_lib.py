@@ -12,9 +12,11 @@ LIB_PATH = os.path.join(_HERE, "libhislam2_b200.so")
 
 HS2_OK, HS2_ERR_INVALID, HS2_ERR_CUDA, HS2_ERR_WORKSPACE, HS2_ERR_DTYPE = range(5)
 HS2_F32, HS2_F16, HS2_BF16, HS2_F64 = range(4)
+HS2_CV_NATIVE, HS2_CV_E4M3 = range(2)
 HS2_DEV_BAD_INDEX = 1
 HS2_DEV_BAD_ETA = 2
 HS2_DEV_TIMEOUT = 4
+HS2_DEV_LIMIT = 8
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int
@@ -29,6 +31,9 @@ SIGNATURES = {
     "hs2_frame_distance": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _i64, _f32, _p, _p, _p],
     "hs2_corr_index_forward": [_p, _i32, _i64, _i32, _i32, _i32, _i32, _p, _i32, _p, _p],
     "hs2_corr_index_backward": [_p, _p, _i32, _i64, _i32, _i32, _i32, _i32, _i32, _p, _p],
+    "hs2_corr_volume_workspace_size": [_i64, _i64, _i32, _i32, _i32, _i32, _i32, ctypes.POINTER(_sz)],
+    "hs2_corr_volume": [_p, _i64, _p, _i64, _i32, _i32, _i32, _i32, _p, _p, _i64, _i32, _i32, _p, _p, _p, _sz,
+                        _p],
     "hs2_altcorr_forward": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _p,
                             _i32, _i32, _p, _p, _p],
     "hs2_altcorr_backward_workspace_size": [_i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32,
@@ -43,6 +48,9 @@ SIGNATURES = {
     "hs2_ba_reduced_system": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32,
                               _i32, _p, _p, _p, _p, _sz, _p],
     "hs2_ba_set_schur_path": [_i32],
+    "hs2_ba_adjoint_workspace_size": [_i64, _i64, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_sz)],
+    "hs2_ba_adjoint": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32, _f32, _f32,
+                       _p, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _sz, _p],
     "hs2_pgba_workspace_size": [_i64, _i64, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_sz)],
     "hs2_pgba": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32,
                  _i32, _f32, _f32, _p, _p, _i64, _p, _p, _sz, _p],
@@ -54,9 +62,24 @@ SIGNATURES = {
     "hs2_profile_enable": [_i32],
     "hs2_launch_count": [],
     "hs2_profile_report": [ctypes.c_char_p, _sz, _i32],
-    "hs2_measure_simt_peaks": [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
     "hs2_ba_keys": [_i64, _i64, _i32, _i32, _p, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _p, _sz, _p],
 }
+
+class BaWindow(ctypes.Structure):
+    """``hs2_ba_window`` of include/hislam2_b200.h (one window of hs2_ba_batch)."""
+    _fields_ = [("poses", _p), ("num_poses", _i64), ("disps", _p), ("num_disps", _i64), ("ht", _i32),
+                ("wd", _i32), ("intrinsics", _p), ("targets", _p), ("weights", _p), ("eta", _p),
+                ("eta_rows", _i64), ("ii", _p), ("jj", _p), ("num_edges", _i64), ("t0", _i32), ("t1", _i32),
+                ("dx", _p), ("dz", _p), ("dz_rows", _i64), ("info", _p)]
+
+
+SIGNATURES.update({
+    "hs2_corr_reproject_lookup": [_p, _i64, _p, _i64, _p, _p, _i32, _i32, _i64, _i32, _i32, _i32, _p, _p, _i64,
+                                  _i32, _p, _p, _p, _p],
+    "hs2_ba_batch_workspace_size": [ctypes.POINTER(BaWindow), _i32, ctypes.POINTER(_sz)],
+    "hs2_ba_batch_prepare": [ctypes.POINTER(BaWindow), _i32, _i32, _i32, _p, _sz, ctypes.POINTER(_i32), _p],
+    "hs2_ba_batch_run": [_p, _i32, _i32, _i32, _f32, _f32, _p],
+})
 
 _lib = None
 
@@ -100,13 +123,6 @@ def profile_report(reset=True):
         name, n, ms = line.split()
         out[name] = (int(n), float(ms))
     return out
-
-
-def measure_simt_peaks():
-    """(fp32, fp64) FMA throughput of the current device in TFLOP/s."""
-    a, b = ctypes.c_double(0), ctypes.c_double(0)
-    check(load().hs2_measure_simt_peaks(ctypes.byref(a), ctypes.byref(b)), "measure_simt_peaks")
-    return a.value, b.value
 
 
 def launch_count():

@@ -51,6 +51,8 @@ def _raise_device_errors(bits, op, indices="ii/jj outside the buffers or >= t1")
         raise RuntimeError("%s: eta must have M or 1 rows (M = number of distinct depth frames)" % op)
     if bits & _lib.HS2_DEV_TIMEOUT:
         raise RuntimeError("%s: a bounded in-kernel wait timed out; the results are not valid" % op)
+    if bits & _lib.HS2_DEV_LIMIT:
+        raise RuntimeError("%s: a kernel size limit was exceeded; the results are not valid" % op)
 
 
 # --------------------------------------------------------------------------- ba
@@ -131,6 +133,136 @@ def ba(poses, disps, intrinsics, *args, disps_sens=None):
     _raise_device_errors(int(h[0]), "ba")
     M = int(h[1])
     return [dx, None if motion_only else dz[:M], None]
+
+
+def ba_adjoint(poses, disps, intrinsics, targets, weights, eta, ii, jj, t0, t1, lm, ep, dx, grad_dx, grad_dz):
+    """Gradients of one ``ba`` iteration (motion_only = False) w.r.t. targets, weights, eta.
+
+    ``poses``/``disps`` are the linearisation point (the state before the step), ``dx``
+    the step's pose update, ``grad_dx`` [t1-t0, 6] and ``grad_dz`` [M, H*W] the incoming
+    gradients of dx and dz.  Returns ``[grad_targets, grad_weights, grad_eta, lam]``
+    (``lam`` [t1-t0, 6]: the adjoint solution of the damped reduced system).  No
+    counterpart in the reference's operator set (its BA is differentiated only on
+    the pure-PyTorch path, hislam2/geom/chol.py:8-22).
+    """
+    _ba_check(poses, disps, intrinsics, targets, weights, eta, ii, jj)
+    eta = eta.contiguous()
+    dev = poses.device
+    t0, t1 = int(t0), int(t1)
+    K, (Kd, ht, wd), E = poses.shape[0], disps.shape, ii.numel()
+    P = t1 - t0
+    for name, t in (("dx", dx), ("grad_dx", grad_dx), ("grad_dz", grad_dz)):
+        _cuda(name, t, dev)
+        _dtype(name, t, torch.float32)
+    dx, grad_dx, grad_dz = dx.contiguous(), grad_dx.contiguous(), grad_dz.contiguous()
+    if tuple(dx.shape) != (P, 6) or tuple(grad_dx.shape) != (P, 6) or grad_dz.dim() != 2 \
+            or grad_dz.shape[1] != ht * wd:
+        raise RuntimeError("ba_adjoint: dx, grad_dx must be [t1-t0, 6] and grad_dz [M, H*W]")
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    _lib.check(lib.hs2_ba_adjoint_workspace_size(K, Kd, ht, wd, E, t0, t1, ctypes.byref(n)),
+               "ba_adjoint_workspace_size")
+    ws = torch.empty(n.value, dtype=torch.uint8, device=dev)
+    gt = torch.empty_like(targets)
+    gw = torch.empty_like(weights)
+    eta_rows = eta.numel() // (ht * wd)
+    ge = torch.empty(eta_rows, ht, wd, dtype=torch.float32, device=dev)
+    lam = torch.zeros(max(P, 0), 6, dtype=torch.float32, device=dev)
+    info = torch.zeros(4, dtype=torch.int32, device=dev)
+    _lib.check(lib.hs2_ba_adjoint(_ptr(poses), K, _ptr(disps), Kd, ht, wd, _ptr(intrinsics), _ptr(targets),
+                                  _ptr(weights), _ptr(eta), eta_rows, _ptr(ii), _ptr(jj), E, t0, t1, float(lm),
+                                  float(ep), _ptr(dx), _ptr(grad_dx), _ptr(grad_dz), grad_dz.shape[0], _ptr(gt),
+                                  _ptr(gw), _ptr(ge), _ptr(lam), _ptr(info), _ptr(ws), n.value, _stream(dev)),
+               "ba_adjoint")
+    h = info.cpu()
+    _raise_device_errors(int(h[0]), "ba_adjoint")
+    if int(h[1]) != grad_dz.shape[0]:
+        raise RuntimeError("ba_adjoint: grad_dz has %d rows, the step has %d depth frames"
+                           % (grad_dz.shape[0], int(h[1])))
+    return [gt, gw, ge.reshape(eta.shape), lam]
+
+
+class BABatch:
+    """Many independent ``ba`` windows solved together (``hs2_ba_batch_*``).
+
+    ``windows``: a list of dicts with the tensors of a ``ba`` call (``poses``,
+    ``disps``, ``intrinsics``, ``targets``, ``weights``, ``eta``, ``ii``, ``jj``) and
+    ``t0``, ``t1``; every window may have its own grid, keyframe and edge count.
+    ``prepare`` (at construction) builds the keys of every window once;
+    :meth:`run` enqueues ``iterations`` LM iterations -- one persistent launch per
+    iteration over all windows -- updating each window's poses / disps in place, and
+    can be captured in a CUDA graph (:meth:`graph`).  The tensors must stay alive and
+    keep their storage while the object is used.  ``gram_split`` / ``ctas_per_sm``
+    are the launch-shape knobs that ``hislam2_b200.autotune`` tunes.
+    """
+
+    def __init__(self, windows, lm, ep, gram_split=4, ctas_per_sm=0):
+        if not windows:
+            raise RuntimeError("ba_batch: no windows")
+        dev = windows[0]["poses"].device
+        self.device, self.lm, self.ep = dev, float(lm), float(ep)
+        self.windows = windows
+        arr = (_lib.BaWindow * len(windows))()
+        self.dx, self.dz, self.info = [], [], []
+        for k, w in enumerate(windows):
+            _ba_check(w["poses"], w["disps"], w["intrinsics"], w["targets"], w["weights"], w["eta"], w["ii"], w["jj"])
+            if w["poses"].device != dev:
+                raise RuntimeError("ba_batch: every window must be on %s" % dev)
+            K, (Kd, ht, wd), E = w["poses"].shape[0], w["disps"].shape, w["ii"].numel()
+            t0, t1 = int(w["t0"]), int(w["t1"])
+            P = t1 - t0
+            S = max(1, min(min(K, Kd), P + E))
+            dx = torch.zeros(max(P, 0), 6, dtype=torch.float32, device=dev)
+            dz = torch.zeros(S, ht * wd, dtype=torch.float32, device=dev)
+            info = torch.zeros(4, dtype=torch.int32, device=dev)
+            self.dx.append(dx)
+            self.dz.append(dz)
+            self.info.append(info)
+            eta = w["eta"]
+            arr[k] = _lib.BaWindow(_ptr(w["poses"]), K, _ptr(w["disps"]), Kd, ht, wd, _ptr(w["intrinsics"]),
+                                   _ptr(w["targets"]), _ptr(w["weights"]), _ptr(eta), eta.numel() // (ht * wd),
+                                   _ptr(w["ii"]), _ptr(w["jj"]), E, t0, t1, _ptr(dx), _ptr(dz), S, _ptr(info))
+        self._arr = arr
+        lib = _lib.load()
+        n = ctypes.c_size_t(0)
+        _lib.check(lib.hs2_ba_batch_workspace_size(arr, len(windows), ctypes.byref(n)), "ba_batch_workspace_size")
+        self.ws = torch.empty(n.value, dtype=torch.uint8, device=dev)
+        grid = ctypes.c_int(0)
+        _lib.check(lib.hs2_ba_batch_prepare(arr, len(windows), int(gram_split), int(ctas_per_sm), _ptr(self.ws),
+                                            n.value, ctypes.byref(grid), _stream(dev)), "ba_batch_prepare")
+        self.grid = grid.value
+        self.check()
+
+    def run(self, iterations):
+        _lib.check(_lib.load().hs2_ba_batch_run(_ptr(self.ws), len(self.windows), self.grid, int(iterations), self.lm,
+                                                self.ep, _stream(self.device)), "ba_batch_run")
+
+    def graph(self, iterations):
+        """A CUDA graph of `iterations` LM iterations (replay with ``.replay()``)."""
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            g.capture_begin()
+            _lib.check(_lib.load().hs2_ba_batch_run(_ptr(self.ws), len(self.windows), self.grid, int(iterations),
+                                                    self.lm, self.ep, _stream(self.device)), "ba_batch_run")
+            g.capture_end()
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        return g
+
+    def check(self):
+        """Raises on device-detected errors of any window; returns each window's M."""
+        out = []
+        for k, info in enumerate(self.info):
+            h = info.cpu()
+            _raise_device_errors(int(h[0]), "ba_batch window %d" % k)
+            out.append(int(h[1]))
+        return out
+
+    def results(self):
+        """[dx, dz] of every window after the last iteration (dz trimmed to M rows)."""
+        Ms = self.check()
+        return [[dx, dz[:M]] for dx, dz, M in zip(self.dx, self.dz, Ms)]
 
 
 def pgba_workspace_bytes(num_poses, num_disps, ht, wd, num_edges, t0, t1):
@@ -446,6 +578,112 @@ def corr_index_backward(volume, coords, corr_grad, radius):
                                                    _ptr(volume_grad), _stream(volume.device)),
                "corr_index_backward")
     return [volume_grad]
+
+
+# ----------------------------------------------------------------- corr_volume
+def corr_volume(fmap1, fmap2, ii=None, jj=None, num_levels=4, precision="native"):
+    """All-pairs correlation pyramid of HI-SLAM2's ``CorrBlock`` on the tensor cores.
+
+    Replaces the caller-side ``CorrBlock.corr`` + ``avg_pool2d`` pyramid
+    (``hislam2/modules/corr.py:29-38,63-71``).  ``fmap1`` [K1,128,H,W] and ``fmap2``
+    [K2,128,H,W] (float16 or bfloat16; a leading [B,N] is flattened); pair e
+    correlates frame ``ii[e]`` of fmap1 with frame ``jj[e]`` of fmap2 (default: frame
+    e with frame e, K1 == K2).  Returns ``num_levels`` tensors [E, H, W, H>>l, W>>l]
+    of the fmaps' dtype: level 0 = (f1/4)^T (f2/4), level l = 2x2 average of level l-1
+    computed as avg_pool2d does.  ``precision="e4m3"`` contracts FP8 e4m3 features with
+    one scale per pixel instead of the 16-bit values.
+    """
+    if fmap1.dim() == 5:
+        fmap1 = fmap1.reshape(-1, *fmap1.shape[2:])
+    if fmap2.dim() == 5:
+        fmap2 = fmap2.reshape(-1, *fmap2.shape[2:])
+    _contig("fmap1", fmap1)
+    _contig("fmap2", fmap2)
+    _cuda("fmap1", fmap1)
+    dev = fmap1.device
+    _cuda("fmap2", fmap2, dev)
+    _dtype("fmap1", fmap1, torch.float16, torch.bfloat16)
+    _dtype("fmap2", fmap2, fmap1.dtype)
+    if fmap1.dim() != 4 or fmap2.dim() != 4 or tuple(fmap1.shape[1:]) != tuple(fmap2.shape[1:]):
+        raise RuntimeError("corr_volume: fmaps [K,C,H,W] of equal C,H,W expected, got %s and %s"
+                           % (tuple(fmap1.shape), tuple(fmap2.shape)))
+    K1, C, H, W = fmap1.shape
+    K2 = fmap2.shape[0]
+    if ii is None or jj is None:
+        if K1 != K2:
+            raise RuntimeError("corr_volume: without ii/jj both fmaps need the same number of frames")
+        ii = jj = torch.arange(K1, device=dev)
+    for name, t in (("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+        _dtype(name, t, torch.int64)
+    ii, jj = ii.contiguous(), jj.contiguous()
+    if ii.numel() != jj.numel():
+        raise RuntimeError("corr_volume: ii and jj differ in length")
+    prec = {"native": _lib.HS2_CV_NATIVE, "e4m3": _lib.HS2_CV_E4M3}.get(precision)
+    if prec is None:
+        raise RuntimeError("corr_volume: precision must be 'native' or 'e4m3'")
+    L = int(num_levels)
+    E = ii.numel()
+    dt = _DTYPES[fmap1.dtype]
+    lib = _lib.load()
+    nbytes = ctypes.c_size_t(0)
+    _lib.check(lib.hs2_corr_volume_workspace_size(K1, K2, C, H, W, dt, prec, ctypes.byref(nbytes)),
+               "corr_volume_workspace_size")
+    pyr = [torch.empty(E, H, W, H >> l, W >> l, dtype=fmap1.dtype, device=dev) for l in range(L)]
+    if E == 0:
+        return pyr
+    ws = torch.empty(max(1, nbytes.value), dtype=torch.uint8, device=dev)
+    ptrs = (ctypes.c_void_p * 4)(*[p.data_ptr() if p.numel() else 0 for p in pyr] + [0] * (4 - L))
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(lib.hs2_corr_volume(_ptr(fmap1), K1, _ptr(fmap2), K2, C, H, W, dt, _ptr(ii), _ptr(jj), E, prec, L,
+                                   ptrs, _ptr(info), _ptr(ws), nbytes.value, _stream(dev)), "corr_volume")
+    bits = int(info.item())
+    if bits:
+        _raise_device_errors(bits, "corr_volume", "ii/jj outside the frames of fmap1/fmap2")
+    return pyr
+
+
+def corr_reproject_lookup(fmap_levels, poses, disps, intrinsics, ii, jj, radius, return_coords=True):
+    """Reprojection + multi-level correlation lookup in one launch.
+
+    Fuses ``DepthVideo.reproject(ii, jj)`` (``hislam2/depth_video.py:170-178``) with the
+    ``AltCorrBlock`` lookup (``hislam2/modules/corr.py:90-117``): ``fmap_levels`` is the
+    list of pooled features [K, C, H>>l, W>>l] (level 0 the features themselves),
+    ``poses`` [K,7], ``disps`` [K,H,W], ``intrinsics`` [4] float32.  Returns ``corr``
+    [E, L*(2r+1)^2, H, W] (the fmaps' dtype) and, with ``return_coords``, the level-0
+    ``coords1`` [E, H, W, 2] (float32).
+    """
+    L = len(fmap_levels)
+    f0 = fmap_levels[0]
+    dev = f0.device
+    for l, f in enumerate(fmap_levels):
+        _contig("fmap_levels[%d]" % l, f)
+        _cuda("fmap_levels[%d]" % l, f, dev)
+        _dtype("fmap_levels[%d]" % l, f, f0.dtype)
+        if f.dim() != 4 or f.shape[:2] != f0.shape[:2] or tuple(f.shape[2:]) != (f0.shape[2] >> l,
+                                                                               f0.shape[3] >> l):
+            raise RuntimeError("corr_reproject_lookup: level %d must be [K, C, H>>%d, W>>%d]" % (l, l, l))
+    for name, t in (("poses", poses), ("disps", disps), ("intrinsics", intrinsics)):
+        _contig(name, t)
+        _cuda(name, t, dev)
+        _dtype(name, t, torch.float32)
+    for name, t in (("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+        _dtype(name, t, torch.int64)
+    ii, jj = ii.contiguous(), jj.contiguous()
+    K, C, H, W = f0.shape
+    if tuple(disps.shape[1:]) != (H, W) or poses.dim() != 2 or poses.shape[1] != 7:
+        raise RuntimeError("corr_reproject_lookup: disps [K,H,W] on the features' grid and poses [K,7] expected")
+    E, r = ii.numel(), int(radius)
+    corr = torch.empty(E, L * (2 * r + 1) ** 2, H, W, dtype=f0.dtype, device=dev)
+    coords = torch.empty(E, H, W, 2, dtype=torch.float32, device=dev) if return_coords else None
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    ptrs = (ctypes.c_void_p * 4)(*[f.data_ptr() for f in fmap_levels] + [0] * (4 - L))
+    _lib.check(_lib.load().hs2_corr_reproject_lookup(_ptr(poses), poses.shape[0], _ptr(disps), disps.shape[0],
+                                                     _ptr(intrinsics), ptrs, L, _DTYPES[f0.dtype], K, C, H, W,
+                                                     _ptr(ii), _ptr(jj), E, r, _ptr(corr), _ptr(coords), _ptr(info),
+                                                     _stream(dev)), "corr_reproject_lookup")
+    return (corr, coords) if return_coords else corr
 
 
 # --------------------------------------------------------------------- altcorr

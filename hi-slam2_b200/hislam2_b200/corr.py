@@ -1,0 +1,168 @@
+"""Correlation blocks of HI-SLAM2 (``hislam2/modules/corr.py``) on the B200 kernels.
+
+* :class:`CorrBlock` keeps the reference's interface (``__init__(fmap1, fmap2,
+  num_levels=4, radius=3)``, ``__call__(coords)``, ``cat``, ``__getitem__``) and its
+  pyramid layout ``[B*N, H, W, H/2^i, W/2^i]``; the pyramid is built by the tensor-core
+  ``corr_volume`` kernel (all pairs + fused avg-pool levels) instead of
+  ``torch.matmul`` + ``F.avg_pool2d`` (reference ``:29-38, :63-71``).
+* :class:`AltCorrBlock` keeps ``AltCorrBlock(fmaps, num_levels=4, radius=3)`` and
+  ``__call__(coords, ii, jj)`` (reference ``:90-117``) on ``altcorr_forward``.
+* :class:`CorrSampler` / :class:`CorrLayer` are the two ``torch.autograd.Function``
+  wrappers.  ``CorrSampler`` is the reference's (``:6-20``).  ``CorrLayer``'s
+  backward is the exact adjoint of the forward (``altcorr_backward`` with
+  ``scale=1/16``): the reference's ``CorrLayer.backward`` cannot run as written
+  (``:83-87`` unpacks three of five saved tensors and returns the wrong number of
+  gradients) and its kernel leaves out the forward's 1/16.
+* :class:`CorrLookup` is the differentiable lookup of the CorrBlock pyramid with
+  respect to the feature maps that stores no pyramid: forward builds the levels
+  with ``corr_volume`` and samples them; backward recomputes the pooled feature
+  pyramid of ``fmap2`` and applies the on-the-fly correlation adjoint
+  (``altcorr_backward``), which equals the pyramid lookup's adjoint because the
+  pooled volume is the correlation with the pooled features.
+"""
+
+import torch
+import torch.nn.functional as F
+
+from . import backends
+
+
+class CorrSampler(torch.autograd.Function):
+    """Bilinear radius-r lookup of one pyramid level; gradient w.r.t. the volume."""
+
+    @staticmethod
+    def forward(ctx, volume, coords, radius):
+        ctx.save_for_backward(volume, coords)
+        ctx.radius = radius
+        corr, = backends.corr_index_forward(volume, coords, radius)
+        return corr
+
+    @staticmethod
+    def backward(ctx, grad_output):
+        volume, coords = ctx.saved_tensors
+        grad_volume, = backends.corr_index_backward(volume, coords, grad_output.contiguous(), ctx.radius)
+        return grad_volume, None, None
+
+
+class CorrBlock:
+    """All-pairs correlation pyramid of HI-SLAM2's frontend (reference ``modules/corr.py:23-71``)."""
+
+    def __init__(self, fmap1, fmap2, num_levels=4, radius=3, precision="native"):
+        self.num_levels = num_levels
+        self.radius = radius
+        batch, num, dim, ht, wd = fmap1.shape
+        levels = backends.corr_volume(fmap1.reshape(batch * num, dim, ht, wd).contiguous(),
+                                      fmap2.reshape(batch * num, dim, ht, wd).contiguous(),
+                                      num_levels=num_levels, precision=precision)
+        self.corr_pyramid = [v.view(batch * num, ht, wd, ht // 2 ** i, wd // 2 ** i) for i, v in enumerate(levels)]
+
+    def __call__(self, coords):
+        out_pyramid = []
+        batch, num, ht, wd, _ = coords.shape
+        coords = coords.permute(0, 1, 4, 2, 3).contiguous().view(batch * num, 2, ht, wd)
+        for i in range(self.num_levels):
+            corr = CorrSampler.apply(self.corr_pyramid[i], (coords / 2 ** i).contiguous(), self.radius)
+            out_pyramid.append(corr.view(batch, num, -1, ht, wd))
+        return torch.cat(out_pyramid, dim=2)
+
+    def cat(self, other):
+        for i in range(self.num_levels):
+            self.corr_pyramid[i] = torch.cat([self.corr_pyramid[i], other.corr_pyramid[i]], 0)
+        return self
+
+    def __getitem__(self, index):
+        for i in range(self.num_levels):
+            self.corr_pyramid[i] = self.corr_pyramid[i][index]
+        return self
+
+
+class CorrLayer(torch.autograd.Function):
+    """On-the-fly radius-r correlation of frames ii of fmap1 with frames jj of fmap2."""
+
+    @staticmethod
+    def forward(ctx, fmap1, fmap2, coords, ii, jj, r):
+        ctx.r = r
+        ctx.save_for_backward(fmap1, fmap2, coords, ii, jj)
+        corr, = backends.altcorr_forward(fmap1, fmap2, coords, ii, jj, r)
+        return corr
+
+    @staticmethod
+    def backward(ctx, grad_corr):
+        fmap1, fmap2, coords, ii, jj = ctx.saved_tensors
+        g1, g2 = backends.altcorr_backward(fmap1, fmap2, coords, ii, jj, grad_corr.float().contiguous(), ctx.r,
+                                           scale=1.0 / 16.0)
+        return g1, g2, None, None, None, None
+
+
+def _pool_pyramid(fmaps, num_levels):
+    """fmaps [B*N, C, H, W] -> list of [B*N, C, H/2^i, W/2^i] (avg_pool2d, floor sizes)."""
+    out = [fmaps]
+    for _ in range(1, num_levels):
+        fmaps = F.avg_pool2d(fmaps, 2, stride=2)
+        out.append(fmaps)
+    return out
+
+
+class AltCorrBlock:
+    """Memory-light correlation of HI-SLAM2's backend (reference ``modules/corr.py:90-117``)."""
+
+    def __init__(self, fmaps, num_levels=4, radius=3):
+        self.num_levels = num_levels
+        self.radius = radius
+        B, N, C, H, W = fmaps.shape
+        levels = _pool_pyramid(fmaps.reshape(B * N, C, H, W), num_levels)
+        self.pyramid = [lv.view(B, N, C, H // 2 ** i, W // 2 ** i) for i, lv in enumerate(levels)]
+
+    def __call__(self, coords, ii, jj):
+        coords = coords.permute(0, 1, 4, 2, 3).contiguous()
+        corr_list = []
+        for i in range(self.num_levels):
+            corr = CorrLayer.apply(self.pyramid[0], self.pyramid[i].contiguous(), (coords / 2 ** i).contiguous(), ii,
+                                   jj, self.radius)
+            corr_list.append(corr.flatten(2, 3))
+        return torch.stack(corr_list, dim=2).flatten(2, 3)
+
+
+class CorrLookup(torch.autograd.Function):
+    """CorrBlock lookup, differentiable w.r.t. both feature maps, without a stored pyramid.
+
+    Inputs: fmap1, fmap2 [B, N, C, H, W] (the gathered frames of each edge), coords
+    [B, N, H, W, 2], radius, num_levels.  Output as ``CorrBlock(fmap1, fmap2)(coords)``:
+    [B, N, L (2r+1)^2, H, W].  Backward saves only the inputs: it pools fmap2 again
+    (levels 1..L-1) and runs the exact adjoint of the on-the-fly correlation on
+    every level, then sends the pooled levels' gradients back through avg_pool2d.
+    """
+
+    @staticmethod
+    def forward(ctx, fmap1, fmap2, coords, radius, num_levels):
+        ctx.save_for_backward(fmap1, fmap2, coords)
+        ctx.radius, ctx.num_levels = radius, num_levels
+        return CorrBlock(fmap1, fmap2, num_levels, radius)(coords)
+
+    @staticmethod
+    def backward(ctx, grad):
+        fmap1, fmap2, coords = ctx.saved_tensors
+        r, L = ctx.radius, ctx.num_levels
+        B, N, C, H, W = fmap1.shape
+        BN = B * N
+        f1 = fmap1.reshape(1, BN, C, H, W).float().contiguous()
+        with torch.enable_grad():
+            f2 = fmap2.reshape(BN, C, H, W).float().detach().requires_grad_(True)
+            levels = _pool_pyramid(f2, L)
+        idx = torch.arange(BN, device=fmap1.device)
+        crd = coords.reshape(1, BN, H, W, 2).permute(0, 1, 4, 2, 3).contiguous()
+        g = grad.reshape(1, BN, L, 2 * r + 1, 2 * r + 1, H, W).float()
+        g1 = torch.zeros_like(f1)
+        g_levels = []
+        for i in range(L):
+            lv = levels[i].detach().reshape(1, BN, C, H // 2 ** i, W // 2 ** i).contiguous()
+            # CorrBlock's channel order is (dx, dy) with dx slowest: the same as altcorr's [.., 2r+1 (x), 2r+1 (y)]
+            gi = g[:, :, i].contiguous()
+            a1, a2 = backends.altcorr_backward(f1, lv, (crd / 2 ** i).contiguous(), idx, idx, gi, r,
+                                               scale=1.0 / 16.0)
+            g1 += a1
+            g_levels.append(a2.reshape(BN, C, H // 2 ** i, W // 2 ** i))
+        with torch.enable_grad():
+            g2, = torch.autograd.grad(levels, [f2], g_levels)
+        return (g1.reshape(fmap1.shape).to(fmap1.dtype), g2.reshape(fmap2.shape).to(fmap2.dtype), None, None,
+                None)

@@ -30,10 +30,12 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <cstdio>
+#include <vector>
 
 #include <cuda.h>
 
-#include "common.cuh"
+#include "ba_common.cuh"
 #include "profile.cuh"
 
 namespace hs2 {
@@ -42,99 +44,6 @@ constexpr int kLinThreads = 128;
 constexpr int kLinPPT = 4;                          // pixels per thread
 constexpr int kLinChunk = kLinThreads * kLinPPT;    // pixels per CTA
 constexpr int kSchurTP = 32;                        // pixels per smem stage
-constexpr int kNB = 64;                             // blocked Cholesky tile
-constexpr int kEtab = 56;                           // floats per edge in the edge table
-
-// ------------------------------------------------------------ workspace ---
-struct BaLayout {
-  size_t flag, slot, kx, gptr, gedge, cursor, rptr, rrow, rpose, sptr, srow, spose, epos, wpos;
-  size_t etab, etab64, hedge, erows, qbuf, wbuf, A, b, x, chol_fail, L11, dinv, ychol, ctl, total;
-};
-
-static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-// Row stride (floats) of the E-row planes: pixels padded to 32 so that every plane
-// row starts on a 128-byte boundary (TMA tiles of 32 pixels).
-static __host__ __device__ __forceinline__ int row_stride(int HW) { return (HW + 31) & ~31; }
-
-static BaLayout ba_layout(int64_t K, int HW, int64_t E, int P, int motion_only) {
-  BaLayout L;
-  const int64_t R = P + E;
-  const int64_t S = std::min<int64_t>(K, R);  // depth-slot capacity
-  const int64_t n = 6 * (int64_t)P;
-  size_t o = 0;
-  auto take = [&](size_t bytes) { size_t at = o; o = align256(o + bytes); return at; };
-  L.flag = take(sizeof(int) * (K + 1));
-  L.slot = take(sizeof(int) * (K + 1));
-  L.kx = take(sizeof(int) * (S + 1));
-  L.gptr = take(sizeof(int) * (S + 2));
-  L.gedge = take(sizeof(int) * (E + 1));
-  L.cursor = take(sizeof(int) * (S + 1));
-  L.rptr = take(sizeof(int) * (S + 2));
-  L.rrow = take(sizeof(int) * (R + 1));
-  L.rpose = take(sizeof(int) * (R + 1));
-  L.sptr = take(sizeof(int) * (S + 2));
-  L.srow = take(sizeof(int) * (R + 1));
-  L.spose = take(sizeof(int) * (R + 1));
-  L.epos = take(sizeof(int) * (E + 1));
-  L.wpos = take(sizeof(int) * (P + 1));
-  L.etab = take(sizeof(float) * kEtab * (E + 1));
-  L.etab64 = take(sizeof(double) * 36 * (E + 1));
-  L.hedge = take(sizeof(double) * 27 * (E + 1));
-  L.erows = take(motion_only ? 0 : sizeof(float) * 6 * (size_t)R * row_stride(HW));
-  L.qbuf = take(motion_only ? 0 : sizeof(float) * (size_t)S * HW);
-  L.wbuf = take(motion_only ? 0 : sizeof(float) * (size_t)S * HW);
-  L.A = take(sizeof(double) * (size_t)(n * n + 1));
-  L.b = take(sizeof(double) * (size_t)(n + 1));
-  L.x = take(sizeof(double) * (size_t)(n + 1));
-  L.chol_fail = take(sizeof(int) * 4);
-  L.L11 = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB * kNB);
-  L.dinv = take(sizeof(double) * (size_t)((n + kNB - 1) / kNB) * kNB);
-  L.ychol = take(sizeof(double) * (size_t)(n + 1));
-  L.ctl = take(sizeof(unsigned) * (4 + 3 * (size_t)((n + kNB - 1) / kNB) +
-                                    (size_t)((n + kNB - 1) / kNB) * ((n + kNB - 1) / kNB)));   // see CholBuf
-  L.total = o;
-  return L;
-}
-
-struct BaPtrs {
-  int *flag, *slot, *kx, *gptr, *gedge, *cursor, *rptr, *rrow, *rpose, *sptr, *srow, *spose, *epos, *wpos;
-  float* etab;
-  double *etab64, *hedge;
-  float *erows, *qbuf, *wbuf;
-  double *A, *b, *x;
-  int* chol_fail;
-};
-
-static BaPtrs ba_ptrs(void* ws, const BaLayout& L) {
-  char* base = static_cast<char*>(ws);
-  BaPtrs p;
-  p.flag = (int*)(base + L.flag);
-  p.slot = (int*)(base + L.slot);
-  p.kx = (int*)(base + L.kx);
-  p.gptr = (int*)(base + L.gptr);
-  p.gedge = (int*)(base + L.gedge);
-  p.cursor = (int*)(base + L.cursor);
-  p.rptr = (int*)(base + L.rptr);
-  p.rrow = (int*)(base + L.rrow);
-  p.rpose = (int*)(base + L.rpose);
-  p.sptr = (int*)(base + L.sptr);
-  p.srow = (int*)(base + L.srow);
-  p.spose = (int*)(base + L.spose);
-  p.epos = (int*)(base + L.epos);
-  p.wpos = (int*)(base + L.wpos);
-  p.etab = (float*)(base + L.etab);
-  p.etab64 = (double*)(base + L.etab64);
-  p.hedge = (double*)(base + L.hedge);
-  p.erows = (float*)(base + L.erows);
-  p.qbuf = (float*)(base + L.qbuf);
-  p.wbuf = (float*)(base + L.wbuf);
-  p.A = (double*)(base + L.A);
-  p.b = (double*)(base + L.b);
-  p.x = (double*)(base + L.x);
-  p.chol_fail = (int*)(base + L.chol_fail);
-  return p;
-}
 
 // ---------------------------------------------------------------- keys ---
 // In-place exclusive scan of data[0..n) by one CTA of 1024 threads; returns the total.
@@ -327,10 +236,10 @@ __global__ void ba_kk_kernel(const int64_t* __restrict__ ii, int E, int t0, int 
 // ---------------------------------------------------------- edge setup ---
 // Six threads per edge: lane c of the group forms column c of L (the FP64 map Ji = L Jj);
 // lane 0 also writes Gij and its rotation matrix.
-__global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int64_t* __restrict__ ii,
-                                     const int64_t* __restrict__ jj, int E, float* __restrict__ etab,
-                                     double* __restrict__ etab64, const int32_t* __restrict__ info) {
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ba_edge_setup_body(int gid, const float* __restrict__ poses,
+                                                   const int64_t* __restrict__ ii, const int64_t* __restrict__ jj,
+                                                   int E, float* __restrict__ etab, double* __restrict__ etab64,
+                                                   const int32_t* __restrict__ info) {
   const int e = gid / 6, c = gid - (gid / 6) * 6;
   if (e >= E || info[0]) return;
   const int64_t a = ii[e], b = jj[e];
@@ -361,64 +270,13 @@ __global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int6
   }
 }
 
-// ------------------------------------------------------------ linearize ---
-// Upper-triangle order of the 21 entries of a symmetric 6x6 block.
-__device__ __forceinline__ int tri6(int r, int c) { return r * 6 - (r * (r - 1)) / 2 + (c - r); }
-
-// Linearisation of one pixel for one edge (reference projective_transform and the
-// per-pixel part of projective_transform_kernel): the point of normalised image
-// coordinates (xn, yn) at disparity h is moved by Gij (tab: t at 0..2, rotation matrix
-// at 44..52) and projected.  Outputs the point Jacobian products of the edge's
-// Hessian block (27 sums: upper triangle of Hjj, then vj) added to H, the Schur
-// terms C (cs) and w (ws), and the row E_j (6).  Pixels closer than kMinDepth
-// contribute nothing but their (zero-weight) residual; a self edge keeps C and w and
-// drops H and E.  The Jacobians have a structural zero each (Ju[1], Jv[0]): those
-// products are never formed.
-__device__ __forceinline__ void lin_pixel(const float* __restrict__ tab, float fx, float fy, float cx, float cy,
-                                          float xn, float yn, float h, float tu, float tv, float wgu, float wgv,
-                                          bool self, float (&H)[32], float& cs, float& ws, float (&Ej)[6]) {
-  const float* R = tab + 44;
-  const float Y0 = fmaf(R[0], xn, fmaf(R[1], yn, R[2])) + h * tab[0];
-  const float Y1 = fmaf(R[3], xn, fmaf(R[4], yn, R[5])) + h * tab[1];
-  const float Y2 = fmaf(R[6], xn, fmaf(R[7], yn, R[8])) + h * tab[2];
-  const bool bad = Y2 < kMinDepth;
-  const float iz = __fdividef(1.0f, Y2);
-  const float xp = fx * (Y0 * iz) + cx;
-  const float yp = fy * (Y1 * iz) + cy;
-  const float z = bad ? 0.f : Y2;
-  const float dd = bad ? 0.f : iz;
-  const float d2 = dd * dd;
-  float wu = bad ? 0.f : 0.001f * wgu;
-  float wv = bad ? 0.f : 0.001f * wgv;
-  const float ru = tu - xp, rv = tv - yp;
-  const float Jp0 = fx * dd, Jp2 = fx * (-Y0 * d2);
-  const float Jp4 = fy * dd, Jp5 = fy * (-Y1 * d2);
-  const float Ju[6] = {Jp0 * h, 0.f, Jp2 * h, Jp2 * Y1, Jp0 * z - Jp2 * Y0, -Jp0 * Y1};
-  const float Jv[6] = {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * Y1, -Jp5 * Y0, Jp4 * Y0};
-  const float Jzu = Jp0 * tab[0] + Jp2 * tab[2];
-  const float Jzv = Jp4 * tab[1] + Jp5 * tab[2];
-  cs += wu * Jzu * Jzu + wv * Jzv * Jzv;
-  ws += wu * ru * Jzu + wv * rv * Jzv;
-  if (self) { wu = 0.f; wv = 0.f; }
-  const float au = wu * ru, av = wv * rv;
-#pragma unroll
-  for (int r = 0; r < 6; ++r) {
-    const float su = wu * Ju[r], sv = wv * Jv[r];
-#pragma unroll
-    for (int c = r; c < 6; ++c) {
-      if (r != 1 && c != 1) H[tri6(r, c)] = fmaf(su, Ju[c], H[tri6(r, c)]);
-      if (r != 0 && c != 0) H[tri6(r, c)] = fmaf(sv, Jv[c], H[tri6(r, c)]);
-    }
-    if (r != 1) H[21 + r] = fmaf(au, Ju[r], H[21 + r]);
-    if (r != 0) H[21 + r] = fmaf(av, Jv[r], H[21 + r]);
-  }
-  const float zu = wu * Jzu, zv = wv * Jzv;
-  Ej[0] = zu * Ju[0];
-  Ej[1] = zv * Jv[1];
-#pragma unroll
-  for (int r = 2; r < 6; ++r) Ej[r] = fmaf(zu, Ju[r], zv * Jv[r]);
+__global__ void ba_edge_setup_kernel(const float* __restrict__ poses, const int64_t* __restrict__ ii,
+                                     const int64_t* __restrict__ jj, int E, float* __restrict__ etab,
+                                     double* __restrict__ etab64, const int32_t* __restrict__ info) {
+  ba_edge_setup_body(blockIdx.x * blockDim.x + threadIdx.x, poses, ii, jj, E, etab, etab64, info);
 }
 
+// ------------------------------------------------------------ linearize ---
 // Sum of v[0..31] over the warp's lanes; lane l returns the total of v[l].  Five
 // exchange rounds halve the vector each time (31 shuffles instead of 5 per value).
 __device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
@@ -436,14 +294,16 @@ __device__ __forceinline__ float warp_transpose_sum(float (&v)[32]) {
   return v[0];
 }
 
-__global__ void __launch_bounds__(kLinThreads, 4)
-ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
-                    const float* __restrict__ targets, const float* __restrict__ weights,
-                    const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj,
-                    int t0, int t1, int motion_only, int skip_fusable, BaPtrs w,
-                    const int32_t* __restrict__ info) {
+// One (depth frame s, pixel chunk) of the linearisation on a CTA of NT threads.
+template <int NT>
+__device__ __forceinline__ void ba_linearize_body(int s, int chunk, const float* __restrict__ disps, int HW, int wd,
+                                                  const float* __restrict__ intr, const float* __restrict__ targets,
+                                                  const float* __restrict__ weights, const float* __restrict__ eta,
+                                                  int64_t eta_rows, const int64_t* __restrict__ jj, int t0, int t1,
+                                                  int motion_only, int skip_fusable, BaPtrs w,
+                                                  const int32_t* __restrict__ info) {
+  constexpr int kChunk = NT * kLinPPT;
   if (info[0]) return;
-  const int s = blockIdx.x;
   const int M = info[1];
   if (s >= M || (skip_fusable && frame_fusable(w, s))) return;
   const int HWs = row_stride(HW);
@@ -452,13 +312,13 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
   const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
 
   __shared__ float tab[kEtab];
-  __shared__ float red[kLinThreads / 32][32];
+  __shared__ float red[NT / 32][32];
 
   int pix[kLinPPT];
   float dsp[kLinPPT], xn[kLinPPT], yn[kLinPPT], Cs[kLinPPT], Ws[kLinPPT], Ei[kLinPPT][6];
 #pragma unroll
   for (int k = 0; k < kLinPPT; ++k) {
-    pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
+    pix[k] = chunk * kChunk + k * NT + threadIdx.x;
     const int pc = pix[k] < HW ? pix[k] : HW - 1;
     dsp[k] = disps[(int64_t)f * HW + pc];
     const int vi = pc / wd;
@@ -521,7 +381,7 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
     if (threadIdx.x < 27) {
       double acc = 0.0;
 #pragma unroll
-      for (int q2 = 0; q2 < kLinThreads / 32; ++q2) acc += (double)red[q2][threadIdx.x];
+      for (int q2 = 0; q2 < NT / 32; ++q2) acc += (double)red[q2][threadIdx.x];
       atomicAdd(&w.hedge[(int64_t)e * 27 + threadIdx.x], acc);
     }
   }
@@ -542,12 +402,22 @@ ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
   }
 }
 
+__global__ void __launch_bounds__(kLinThreads, 4)
+ba_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
+                    const float* __restrict__ targets, const float* __restrict__ weights,
+                    const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj,
+                    int t0, int t1, int motion_only, int skip_fusable, BaPtrs w,
+                    const int32_t* __restrict__ info) {
+  ba_linearize_body<kLinThreads>(blockIdx.x, blockIdx.y, disps, HW, wd, intr, targets, weights, eta, eta_rows, jj, t0,
+                                 t1, motion_only, skip_fusable, w, info);
+}
+
 // ------------------------------------------------------------- assemble ---
 // Six threads per edge: lane r of the group adds row r of Hjj / vj (block j), of
 // Hii = L Hjj L^T / vi = L vj (block i) and of Hij = L Hjj (lower block triangle).
-__global__ void ba_assemble_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, int E, int t0,
-                                   int P, BaPtrs w, const int32_t* __restrict__ info) {
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ba_assemble_body(int gid, const int64_t* __restrict__ ii,
+                                                 const int64_t* __restrict__ jj, int E, int t0, int P, BaPtrs w,
+                                                 const int32_t* __restrict__ info) {
   const int e = gid / 6, r = gid - (gid / 6) * 6;
   if (e >= E || info[0]) return;
   const int i = (int)(ii[e] - t0), j = (int)(jj[e] - t0);
@@ -610,6 +480,11 @@ __global__ void ba_assemble_kernel(const int64_t* __restrict__ ii, const int64_t
   }
 }
 
+__global__ void ba_assemble_kernel(const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, int E, int t0,
+                                   int P, BaPtrs w, const int32_t* __restrict__ info) {
+  ba_assemble_body(blockIdx.x * blockDim.x + threadIdx.x, ii, jj, E, t0, P, w, info);
+}
+
 // ---------------------------------------------------------------- schur ---
 // Per (depth frame k, pixel chunk): S_ab = sum_p Q E_a E_b^T for every pair of the
 // frame's Schur rows a <= b (6x6 blocks) and v_a = sum_p Q w E_a.  Rows are
@@ -648,16 +523,15 @@ __device__ __forceinline__ void schur_scatter_block(double* A, int64_t n, int pa
   }
 }
 
-__global__ void __launch_bounds__(256)
-ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, int skip_fusable,
-                const int32_t* __restrict__ info) {
+// One (depth frame s, pixel split) of the SIMT Schur Gram on a CTA of 256 threads.
+__device__ __forceinline__ void ba_schur_body(int s, int split, int HW, int chunk, BaPtrs w, int P, int min_blocks,
+                                              int skip_fusable, const int32_t* __restrict__ info) {
   if (info[0]) return;
-  const int s = blockIdx.x;
   if (s >= info[1] || (skip_fusable && frame_fusable(w, s))) return;
   const int r0 = w.sptr[s];
   const int nr = w.sptr[s + 1] - r0;
   if (nr == 0 || nr < min_blocks) return;
-  const int c0 = blockIdx.y * chunk;
+  const int c0 = split * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
   const int* spose = w.spose + r0;
@@ -767,6 +641,12 @@ ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, int skip_fus
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(256)
+ba_schur_kernel(int HW, int chunk, BaPtrs w, int P, int min_blocks, int skip_fusable,
+                const int32_t* __restrict__ info) {
+  ba_schur_body(blockIdx.x, blockIdx.y, HW, chunk, w, P, min_blocks, skip_fusable, info);
 }
 
 // Mirrors the lower triangle of the reduced system into the upper one (diagnostics only).
@@ -2108,11 +1988,12 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
 }
 
 // -------------------------------------------------------------- backsub ---
-__global__ void __launch_bounds__(kLinThreads)
-ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const float* __restrict__ dx,
-                  float* __restrict__ dz, int64_t dz_rows, const int32_t* __restrict__ info) {
+template <int NT>
+__device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restrict__ disps, int HW, int P, BaPtrs w,
+                                                const float* __restrict__ dx, float* __restrict__ dz,
+                                                int64_t dz_rows, const int32_t* __restrict__ info) {
+  constexpr int kChunk = NT * kLinPPT;
   if (info[0]) return;
-  const int s = blockIdx.x;
   if (s >= info[1] || s >= dz_rows) return;
   const int f = w.kx[s];
   const int r0 = w.rptr[s], r1 = w.rptr[s + 1];
@@ -2123,13 +2004,13 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
   int pix[kLinPPT];
 #pragma unroll
   for (int k = 0; k < kLinPPT; ++k) {
-    pix[k] = blockIdx.y * kLinChunk + k * kLinThreads + threadIdx.x;
+    pix[k] = chunk * kChunk + k * NT + threadIdx.x;
     acc[k] = 0.f;
   }
   for (int rb = r0; rb < r1; rb += kRows) {
     const int nrw = min(kRows, r1 - rb);
     __syncthreads();
-    for (int i = threadIdx.x; i < nrw * 6; i += kLinThreads) {
+    for (int i = threadIdx.x; i < nrw * 6; i += NT) {
       const int ix = w.rpose[rb + i / 6];
       // reference EvT6x1_kernel skips rows of pose index <= 0
       xs[i / 6][i % 6] = (ix <= 0 || ix >= P) ? 0.f : dx[ix * 6 + i % 6];
@@ -2162,11 +2043,16 @@ ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
   }
 }
 
+__global__ void __launch_bounds__(kLinThreads)
+ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const float* __restrict__ dx,
+                  float* __restrict__ dz, int64_t dz_rows, const int32_t* __restrict__ info) {
+  ba_backsub_body<kLinThreads>(blockIdx.x, blockIdx.y, disps, HW, P, w, dx, dz, dz_rows, info);
+}
+
 // ------------------------------------------------------------ pose retr ---
-__global__ void ba_pose_retr_kernel(float* __restrict__ poses, int t0, int P, const BaPtrs w,
-                                    const int32_t* __restrict__ info) {
+__device__ __forceinline__ void ba_pose_retr_body(int k, float* __restrict__ poses, int t0, int P, const BaPtrs w,
+                                                  const int32_t* __restrict__ info) {
   if (info[0]) return;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= P) return;
   float* p = poses + 7 * (int64_t)(t0 + k);
   double t[3] = {p[0], p[1], p[2]};
@@ -2176,6 +2062,11 @@ __global__ void ba_pose_retr_kernel(float* __restrict__ poses, int t0, int P, co
   retract_left(xi, t, q);
   for (int c = 0; c < 3; ++c) p[c] = (float)t[c];
   for (int c = 0; c < 4; ++c) p[3 + c] = (float)q[c];
+}
+
+__global__ void ba_pose_retr_kernel(float* __restrict__ poses, int t0, int P, const BaPtrs w,
+                                    const int32_t* __restrict__ info) {
+  ba_pose_retr_body(blockIdx.x * blockDim.x + threadIdx.x, poses, t0, P, w, info);
 }
 
 // ------------------------------------------------------------ host side ---
@@ -2519,6 +2410,348 @@ extern "C" int hs2_ba_set_schur_path(int path) {
   g_schur_path.store(path);
   return HS2_OK;
 }
+
+namespace hs2 {
+
+// ============================================================ LM adjoint ===
+// Adjoint of ONE Levenberg-Marquardt step of ba (motion_only = 0) with respect to
+// targets, weights and eta at a fixed linearisation point (poses, disparities):
+// implicit differentiation through the damped Schur solve.  With the step written
+// as the damped system M_d [dx; dz] = [b; gd] (pose block A + ep + lm diag(R),
+// R = A - E Q E^T, depth block C + eta, Q = 1/(C + eta)) and the reference's
+// back-substitution dz = Q (gd - E~^T dx) (E~ without the rows of window pose 0,
+// EvT6x1_kernel's ix <= 0 skip), the adjoint of (gdx, gdz) is
+//   lam   = R_d^-1 (gdx - E~ Q gdz)                          (the forward's Cholesky)
+//   per depth pixel k, with s_lam = E_k . lam, s_x = E_k . dx, s~_x = E~_k . dx and
+//   e2 = sum over pose dofs of lam dx E_k^2 (E_k summed over rows of one pose):
+//     Qbar  = gdz (gd - s~_x) - s_lam gd + s_lam s_x + lm e2
+//     gdbar = Q (gdz - s_lam),   Cbar = etabar = -Q^2 Qbar
+//   per edge-pixel and channel, with u = J . lam, v = J . dx, v~ (without pose 0),
+//   J_d the depth Jacobian, r the residual and w' = 0.001 weight (0 when z < MIN_DEPTH):
+//     wbar' = -u v - lm sum lam dx J^2 + u r
+//             + J_d Q (-gdz v~ - gd u + s_x u + s_lam v + 2 lm sum J lam dx E)   (pose terms)
+//             + Cbar J_d^2 + gdbar J_d r                                          (depth terms)
+//     weights_bar = 0.001 valid wbar',  targets_bar = w' u + gdbar w' J_d
+// (self-edges keep only the depth terms, as in the forward).  R_bar = -lam dx^T -
+// lm diag(lam dx) is rank two plus a diagonal, which is why every term above needs
+// only the per-pixel scalars and no second Gram.
+constexpr int kAdjThreads = 128;
+constexpr int kAdjMaxRows = 256;     // Schur rows of one depth frame held in shared memory
+
+// rhs[a*6+x] = sum over Schur rows of pose a >= 1 of sum_p E Q gdz (FP64 accumulation)
+__global__ void __launch_bounds__(kAdjThreads)
+ba_adj_rhs_kernel(int HW, BaPtrs w, const float* __restrict__ gdz, double* __restrict__ acc,
+                  const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  if (s >= info[1]) return;
+  const int HWs = row_stride(HW);
+  const int q0 = w.sptr[s], q1 = w.sptr[s + 1];
+  __shared__ float red[kAdjThreads / 32][6];
+  for (int q = q0; q < q1; ++q) {
+    const int pose = w.spose[q];
+    if (pose < 1) continue;
+    const int r = w.rptr[s] + (q - q0);
+    float part[6] = {0, 0, 0, 0, 0, 0};
+    for (int p = blockIdx.y * blockDim.x + threadIdx.x; p < HW; p += gridDim.y * blockDim.x) {
+      const float qz = w.qbuf[(int64_t)s * HW + p] * gdz[(int64_t)s * HW + p];
+#pragma unroll
+      for (int x = 0; x < 6; ++x) part[x] = fmaf(w.erows[((int64_t)r * 6 + x) * HWs + p], qz, part[x]);
+    }
+#pragma unroll
+    for (int x = 0; x < 6; ++x) part[x] = warp_sum(part[x]);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+      for (int x = 0; x < 6; ++x) red[threadIdx.x >> 5][x] = part[x];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      double t = 0.0;
+      for (int k = 0; k < kAdjThreads / 32; ++k) t += red[k][threadIdx.x];
+      atomicAdd(&acc[pose * 6 + threadIdx.x], t);
+    }
+  }
+}
+
+__global__ void ba_adj_b_kernel(int n, const float* __restrict__ gdx, const double* __restrict__ acc,
+                                double* __restrict__ b, const int32_t* __restrict__ info) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || info[0]) return;
+  b[i] = (double)gdx[i] - acc[i];
+}
+
+// Per depth pixel: s_lam, s_x, gdbar, Cbar (stored for the edge kernel) and etabar.
+__global__ void __launch_bounds__(kAdjThreads)
+ba_adj_pixel_kernel(int HW, BaPtrs w, const float* __restrict__ lam, const float* __restrict__ dx,
+                    const float* __restrict__ gdz, float lm, int64_t eta_rows, float* __restrict__ pix,
+                    float* __restrict__ geta, const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int s = blockIdx.x;
+  const int M = info[1];
+  if (s >= M) return;
+  const int HWs = row_stride(HW);
+  const int q0 = w.sptr[s], nq = min(w.sptr[s + 1] - q0, kAdjMaxRows);
+  if (w.sptr[s + 1] - q0 > kAdjMaxRows) {
+    if (threadIdx.x == 0 && blockIdx.y == 0) atomicOr((int32_t*)info, HS2_DEV_LIMIT);
+    return;
+  }
+  __shared__ int pose[kAdjMaxRows], first[kAdjMaxRows], nxt[kAdjMaxRows];
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) pose[q] = w.spose[q0 + q];
+  __syncthreads();
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+    int f = 1, n = -1;
+    for (int k = 0; k < q; ++k) f &= pose[k] != pose[q];
+    for (int k = nq - 1; k > q; --k)
+      if (pose[k] == pose[q]) n = k;
+    first[q] = f;
+    nxt[q] = n;
+  }
+  __syncthreads();
+  const int rbase = w.rptr[s];
+  const int p = blockIdx.y * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  float sl = 0.f, sx = 0.f, sxt = 0.f, e2 = 0.f;
+  for (int q = 0; q < nq; ++q) {
+    if (!first[q]) continue;
+    const int a = pose[q];
+    float e[6];
+#pragma unroll
+    for (int x = 0; x < 6; ++x) e[x] = 0.f;
+    for (int k = q; k >= 0; k = nxt[k]) {
+#pragma unroll
+      for (int x = 0; x < 6; ++x) e[x] += w.erows[((int64_t)(rbase + k) * 6 + x) * HWs + p];
+    }
+#pragma unroll
+    for (int x = 0; x < 6; ++x) {
+      const float l = lam[a * 6 + x], d = dx[a * 6 + x];
+      sl = fmaf(e[x], l, sl);
+      sx = fmaf(e[x], d, sx);
+      if (a >= 1) sxt = fmaf(e[x], d, sxt);
+      e2 = fmaf(l * d, e[x] * e[x], e2);
+    }
+  }
+  const int64_t k = (int64_t)s * HW + p;
+  const float Q = w.qbuf[k], gd = w.wbuf[k], zb = gdz[k];
+  const float Qbar = zb * (gd - sxt) - sl * gd + sl * sx + lm * e2;
+  const float gdbar = Q * (zb - sl);
+  const float Cbar = -Q * Q * Qbar;
+  const int64_t MHW = (int64_t)M * HW;
+  pix[k] = sl;
+  pix[MHW + k] = sx;
+  pix[2 * MHW + k] = gdbar;
+  pix[3 * MHW + k] = Cbar;
+  if (eta_rows == 1) atomicAdd(&geta[p], Cbar);
+  else geta[k] = Cbar;
+}
+
+// Per edge-pixel: the linearisation again (lin_pixel's arithmetic), then the
+// gradients of the edge's targets and weights.
+__global__ void __launch_bounds__(kAdjThreads)
+ba_adj_edge_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
+                   const float* __restrict__ targets, const float* __restrict__ weights,
+                   const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, int t0, int P, BaPtrs w,
+                   const float* __restrict__ lam, const float* __restrict__ dx, const float* __restrict__ gdz,
+                   float lm, const float* __restrict__ pix, float* __restrict__ gt, float* __restrict__ gw,
+                   const int32_t* __restrict__ info) {
+  if (info[0]) return;
+  const int e = blockIdx.x;
+  const int M = info[1];
+  const int HWs = row_stride(HW);
+  __shared__ float tab[kEtab];
+  __shared__ float sl_a[6], sd_a[6], sl_b[6], sd_b[6];
+  __shared__ int rows_a[8], rows_b[8], nra, nrb;
+  const int f = (int)ii[e], g = (int)jj[e];
+  const int s = w.slot[f];
+  const int a = f - t0, b = g - t0;
+  const bool ina = a >= 0 && a < P, inb = b >= 0 && b < P, self = f == g;
+  if (threadIdx.x < kEtab) tab[threadIdx.x] = w.etab[(int64_t)e * kEtab + threadIdx.x];
+  if (threadIdx.x < 6) {
+    sl_a[threadIdx.x] = ina ? lam[a * 6 + threadIdx.x] : 0.f;
+    sd_a[threadIdx.x] = ina ? dx[a * 6 + threadIdx.x] : 0.f;
+    sl_b[threadIdx.x] = inb ? lam[b * 6 + threadIdx.x] : 0.f;
+    sd_b[threadIdx.x] = inb ? dx[b * 6 + threadIdx.x] : 0.f;
+  }
+  if (threadIdx.x == 0) {
+    // storage rows of pose a and pose b among the Schur rows of the edge's depth frame
+    int na = 0, nb = 0;
+    const int q0 = w.sptr[s], q1 = w.sptr[s + 1];
+    for (int q = q0; q < q1; ++q) {
+      const int pz = w.spose[q];
+      if (pz == a) {
+        if (na < 8) rows_a[na] = w.rptr[s] + (q - q0);
+        ++na;
+      }
+      if (pz == b) {
+        if (nb < 8) rows_b[nb] = w.rptr[s] + (q - q0);
+        ++nb;
+      }
+    }
+    if ((na > 8 || nb > 8) && blockIdx.y == 0) atomicOr((int32_t*)info, HS2_DEV_LIMIT);
+    na = min(na, 8);
+    nb = min(nb, 8);
+    nra = na;
+    nrb = nb;
+  }
+  __syncthreads();
+  const int p = blockIdx.y * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  const float fx = intr[0], fy = intr[1], cx = intr[2], cy = intr[3];
+  const int vi = p / wd;
+  const float xn = ((float)(p - vi * wd) - cx) / fx, yn = ((float)vi - cy) / fy;
+  const float h = disps[(int64_t)f * HW + p];
+  const float* R = tab + 44;
+  const float Y0 = fmaf(R[0], xn, fmaf(R[1], yn, R[2])) + h * tab[0];
+  const float Y1 = fmaf(R[3], xn, fmaf(R[4], yn, R[5])) + h * tab[1];
+  const float Y2 = fmaf(R[6], xn, fmaf(R[7], yn, R[8])) + h * tab[2];
+  const bool bad = Y2 < kMinDepth;
+  const float iz = __fdividef(1.0f, Y2);
+  const float proj[2] = {fx * (Y0 * iz) + cx, fy * (Y1 * iz) + cy};
+  const float z = bad ? 0.f : Y2, dd = bad ? 0.f : iz, d2 = dd * dd;
+  const float Jp0 = fx * dd, Jp2 = fx * (-Y0 * d2), Jp4 = fy * dd, Jp5 = fy * (-Y1 * d2);
+  const float Jc[2][6] = {{Jp0 * h, 0.f, Jp2 * h, Jp2 * Y1, Jp0 * z - Jp2 * Y0, -Jp0 * Y1},
+                          {0.f, Jp4 * h, Jp5 * h, -Jp4 * z + Jp5 * Y1, -Jp5 * Y0, Jp4 * Y0}};
+  const float Jd[2] = {Jp0 * tab[0] + Jp2 * tab[2], Jp4 * tab[1] + Jp5 * tab[2]};
+  float Ea[6], Eb[6];
+#pragma unroll
+  for (int x = 0; x < 6; ++x) { Ea[x] = 0.f; Eb[x] = 0.f; }
+  for (int k = 0; k < nra; ++k)
+#pragma unroll
+    for (int x = 0; x < 6; ++x) Ea[x] += w.erows[((int64_t)rows_a[k] * 6 + x) * HWs + p];
+  for (int k = 0; k < nrb; ++k)
+#pragma unroll
+    for (int x = 0; x < 6; ++x) Eb[x] += w.erows[((int64_t)rows_b[k] * 6 + x) * HWs + p];
+  const int64_t kp = (int64_t)s * HW + p;
+  const int64_t MHW = (int64_t)M * HW;
+  const float sl = pix[kp], sx = pix[MHW + kp], gdbar = pix[2 * MHW + kp], Cbar = pix[3 * MHW + kp];
+  const float Q = w.qbuf[kp], gd = w.wbuf[kp], zb = gdz[kp];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int64_t o = ((int64_t)e * 2 + c) * HW + p;
+    const float wgt = bad ? 0.f : 0.001f * weights[o];
+    const float r = targets[o] - proj[c];
+    // Ji = L Jj (L from the edge table, as the forward's Ei = L Ej)
+    float Ji[6];
+#pragma unroll
+    for (int x = 0; x < 6; ++x) {
+      float t = 0.f;
+#pragma unroll
+      for (int y = 0; y < 6; ++y) t = fmaf(tab[8 + x * 6 + y], Jc[c][y], t);
+      Ji[x] = t;
+    }
+    float u = 0.f, v = 0.f, vt = 0.f, dmp = 0.f, eb = 0.f;
+#pragma unroll
+    for (int x = 0; x < 6; ++x) {
+      const float ja = ina ? Ji[x] : 0.f, jb = inb ? Jc[c][x] : 0.f;
+      u += ja * sl_a[x] + jb * sl_b[x];
+      v += ja * sd_a[x] + jb * sd_b[x];
+      vt += (a >= 1 ? ja * sd_a[x] : 0.f) + (b >= 1 ? jb * sd_b[x] : 0.f);
+      dmp += ja * ja * sl_a[x] * sd_a[x] + jb * jb * sl_b[x] * sd_b[x];
+      eb += ja * sl_a[x] * sd_a[x] * Ea[x] + jb * sl_b[x] * sd_b[x] * Eb[x];
+    }
+    float wb = Cbar * Jd[c] * Jd[c] + gdbar * Jd[c] * r;
+    float tb = gdbar * wgt * Jd[c];
+    if (!self) {
+      wb += -u * v - lm * dmp + u * r + Jd[c] * Q * (-zb * vt - gd * u + sx * u + sl * v + 2.f * lm * eb);
+      tb += wgt * u;
+    }
+    gw[o] = bad ? 0.f : 0.001f * wb;
+    gt[o] = tb;
+  }
+}
+
+static size_t ba_adj_extra(int64_t M, int HW, int P) {
+  return align256(sizeof(double) * (6 * (size_t)P + 1)) + align256(sizeof(float) * (6 * (size_t)P + 1)) +
+         align256(sizeof(float) * 4 * (size_t)M * HW);
+}
+
+}  // namespace hs2
+
+extern "C" int hs2_ba_adjoint_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd,
+                                             int64_t num_edges, int t0, int t1, size_t* bytes) {
+  using namespace hs2;
+  if (!bytes) {
+    set_error("ba_adjoint_workspace_size: null output");
+    return HS2_ERR_INVALID;
+  }
+  BaProblem p = make_problem(num_poses, num_disps, ht, wd, num_edges, t0, t1, 0);
+  int rc = ba_check(p, "ba_adjoint_workspace_size");
+  if (rc) return rc;
+  const int64_t S = std::min<int64_t>(p.K, (int64_t)p.P + p.E);
+  *bytes = ba_layout(p.K, p.HW, p.E, p.P, 0).total + ba_adj_extra(S, p.HW, p.P);
+  return HS2_OK;
+}
+
+extern "C" int hs2_ba_adjoint(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht,
+                              int wd, const float* intrinsics, const float* targets, const float* weights,
+                              const float* eta, int64_t eta_rows, const int64_t* ii, const int64_t* jj,
+                              int64_t num_edges, int t0, int t1, float lm, float ep, const float* dx,
+                              const float* grad_dx, const float* grad_dz, int64_t dz_rows, float* grad_targets,
+                              float* grad_weights, float* grad_eta, float* lam, int32_t* info, void* workspace,
+                              size_t workspace_bytes, hs2_stream_t stream) {
+  using namespace hs2;
+  BaProblem p = make_problem(num_poses, num_disps, ht, wd, num_edges, t0, t1, 0);
+  int rc = ba_check(p, "ba_adjoint");
+  if (rc) return rc;
+  const BaLayout L = ba_layout(p.K, p.HW, p.E, p.P, 0);
+  const int64_t S = std::min<int64_t>(p.K, (int64_t)p.P + p.E);
+  const size_t need = L.total + ba_adj_extra(S, p.HW, p.P);
+  if (!workspace || workspace_bytes < need) {
+    set_error("ba_adjoint: workspace of %zu bytes required", need);
+    return HS2_ERR_WORKSPACE;
+  }
+  if (!lam || !info || (p.E > 0 && (!grad_targets || !grad_weights)) || !grad_eta || (p.P > 0 && (!dx || !grad_dx))) {
+    set_error("ba_adjoint: null output or input pointer");
+    return HS2_ERR_INVALID;
+  }
+  if ((rc = bind_device(poses))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  BaPtrs w = ba_ptrs(workspace, L);
+  char* extra = static_cast<char*>(workspace) + L.total;
+  double* acc = reinterpret_cast<double*>(extra);
+  float* pix = reinterpret_cast<float*>(extra + align256(sizeof(double) * (6 * (size_t)p.P + 1)) +
+                                        align256(sizeof(float) * (6 * (size_t)p.P + 1)));
+  if ((rc = run_keys(p, ii, jj, eta_rows, w, info, s))) return rc;
+  const int P = p.P;
+  const int n = 6 * P;
+  HS2_CUDA(cudaMemsetAsync(grad_eta, 0, sizeof(float) * (size_t)eta_rows * p.HW, s));
+  if (p.E > 0) {
+    HS2_CUDA(cudaMemsetAsync(grad_targets, 0, sizeof(float) * 2 * (size_t)p.E * p.HW, s));
+    HS2_CUDA(cudaMemsetAsync(grad_weights, 0, sizeof(float) * 2 * (size_t)p.E * p.HW, s));
+  }
+  if (S == 0) return HS2_OK;
+  const BaLaunch l = ba_launch_shape(p);
+  if ((rc = build_system(p, l, poses, disps, intrinsics, targets, weights, eta, eta_rows, ii, jj, w, info, s)))
+    return rc;
+  const int chunks = (p.HW + kAdjThreads - 1) / kAdjThreads;
+  if (n > 0) {
+    HS2_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * n, s));
+    HS2_PROF("ba_adj_rhs", s);
+    ba_adj_rhs_kernel<<<dim3((unsigned)S, std::min(chunks, 8)), kAdjThreads, 0, s>>>(p.HW, w, grad_dz, acc, info);
+    HS2_LAUNCH_CHECK("ba_adj_rhs_kernel");
+    ba_adj_b_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, grad_dx, acc, w.b, info);
+    HS2_LAUNCH_CHECK("ba_adj_b_kernel");
+    char* wsb = static_cast<char*>(workspace);
+    CholBuf cb{(double*)(wsb + L.L11), (double*)(wsb + L.dinv), (double*)(wsb + L.ychol), (unsigned*)(wsb + L.ctl)};
+    if ((rc = run_cholesky(n, lm, ep, w, cb, lam, info, s))) return rc;
+  }
+  {
+    HS2_PROF("ba_adj_pixel", s);
+    ba_adj_pixel_kernel<<<dim3((unsigned)S, chunks), kAdjThreads, 0, s>>>(p.HW, w, lam, dx, grad_dz, lm, eta_rows,
+                                                                         pix, grad_eta, info);
+    HS2_LAUNCH_CHECK("ba_adj_pixel_kernel");
+  }
+  if (p.E > 0) {
+    HS2_PROF("ba_adj_edge", s);
+    ba_adj_edge_kernel<<<dim3((unsigned)p.E, chunks), kAdjThreads, 0, s>>>(
+        disps, p.HW, p.wd, intrinsics, targets, weights, ii, jj, t0, P, w, lam, dx, grad_dz, lm, pix, grad_targets,
+        grad_weights, info);
+    HS2_LAUNCH_CHECK("ba_adj_edge_kernel");
+  }
+  return HS2_OK;
+}
+
+namespace hs2 {
+
+}  // namespace hs2
 
 // ================================================================= pgba ===
 // Sim3 pose-graph bundle adjustment (reference operator: src/droid.cpp:171-196 ->
@@ -3110,3 +3343,6 @@ extern "C" int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int
   }
   return HS2_OK;
 }
+
+#include <vector>
+#include "ba_batch.cuh"

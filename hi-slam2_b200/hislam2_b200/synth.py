@@ -243,3 +243,41 @@ def make_pgba_problem(name="frontend_small", seed=0, device="cpu", num_factors=N
     out = {k: (v.to(device) if isinstance(v, torch.Tensor) else v) for k, v in out.items()}
     out["Hsp"], out["vsp"] = out["Hsp"].contiguous(), out["vsp"].contiguous()
     return out
+
+
+def make_batch_problems(num_windows=64, seed=0, device="cpu"):
+    """The batching workload: ``num_windows`` independent BA windows of uneven sizes --
+    keyframes U{8..40}, edges U{20..500} (capped by the K(K-1) ordered pairs), a 43x77
+    or 30x40 grid -- each drawn like the frontend window (|i-j| <= 3 pairs first, then
+    random pairs), t0 = 1, lm = 1e-4, ep = 0.1.  Returns a list of ``ba`` input dicts."""
+    g = torch.Generator().manual_seed(seed + 3000)
+    out = []
+    for w in range(num_windows):
+        K = int(torch.randint(8, 41, (1,), generator=g))
+        E = int(torch.randint(20, 501, (1,), generator=g))
+        ht, wd, img = (43, 77, (344, 616)) if int(torch.randint(0, 2, (1,), generator=g)) == 0 else (30, 40, (240, 320))
+        pairs = [(i, j) for i in range(K) for j in range(K) if i != j]
+        near = [p for p in pairs if abs(p[0] - p[1]) <= 3]
+        far = [p for p in pairs if abs(p[0] - p[1]) > 3]
+        perm = torch.randperm(len(far), generator=g).tolist()
+        e = (near + [far[k] for k in perm])[:min(E, len(pairs))]
+        intr = intrinsics_for(img)
+        xi = 0.05 * torch.randn(K, 6, generator=g, dtype=torch.float64)
+        poses_gt = se3_exp(xi)
+        disps_gt = 0.1 + 1.9 * torch.rand(K, ht, wd, generator=g, dtype=torch.float64)
+        ii = torch.tensor([a for a, _ in e], dtype=torch.int64)
+        jj = torch.tensor([b for _, b in e], dtype=torch.int64)
+        coords = reproject(poses_gt, disps_gt, intr, ii, jj)
+        targets = coords + 0.5 * torch.randn(coords.shape, generator=g, dtype=torch.float64)
+        weights = torch.rand(len(e), ht, wd, 2, generator=g, dtype=torch.float64)
+        t0 = 1
+        poses = poses_gt.clone()
+        pert = se3_exp(0.01 * torch.randn(K, 6, generator=g, dtype=torch.float64))
+        poses[t0:] = pose_compose(pert[t0:], poses_gt[t0:])
+        f32 = dict(dtype=torch.float32, device=device)
+        out.append(dict(poses=poses.to(**f32).contiguous(), disps=disps_gt.to(**f32).contiguous(),
+                        intrinsics=intr.to(**f32), targets=targets.permute(0, 3, 1, 2).to(**f32).contiguous(),
+                        weights=weights.permute(0, 3, 1, 2).to(**f32).contiguous(),
+                        eta=torch.full((K, ht, wd), 1e-3, **f32), ii=ii.to(device), jj=jj.to(device), t0=t0, t1=K,
+                        iters=4, lm=1e-4, ep=0.1))
+    return out

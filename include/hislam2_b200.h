@@ -39,7 +39,8 @@ enum hs2_dtype { HS2_F32 = 0, HS2_F16 = 1, HS2_BF16 = 2, HS2_F64 = 3 };
 enum hs2_device_error {
   HS2_DEV_BAD_INDEX = 1, /* an edge index lies outside the pose/disparity buffers or >= t1 */
   HS2_DEV_BAD_ETA = 2,   /* eta has neither M nor 1 rows (M = #distinct depth frames) */
-  HS2_DEV_TIMEOUT = 4    /* a bounded wait inside a kernel gave up (results are not valid) */
+  HS2_DEV_TIMEOUT = 4,   /* a bounded wait inside a kernel gave up (results are not valid) */
+  HS2_DEV_LIMIT = 8      /* a per-kernel size limit was exceeded (results are not valid) */
 };
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -73,6 +74,117 @@ int hs2_corr_index_forward(const void* volume, int dtype, int64_t n, int h1, int
  */
 int hs2_corr_index_backward(const float* coords, const void* corr_grad, int dtype, int64_t n, int h1,
                             int w1, int h2, int w2, int radius, void* volume_grad, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * ba_batch  (callers: hislam2/factor_graph.py:190-235 runs one ba per window;
+ * this solves many independent windows at once, each with the semantics of
+ * hs2_ba / src/droid_kernels.cu:1820-1937)
+ *   One hs2_ba_window per window, with its own device buffers and sizes (any grid,
+ *   keyframe and edge count; at most 256 optimised poses).  motion_only is not
+ *   supported.  hs2_ba_batch_prepare (synchronous on `stream`, not for capture)
+ *   builds the plan and each window's keys in the workspace and returns the grid of
+ *   the persistent launch; the window list must not change afterwards.
+ *   hs2_ba_batch_run enqueues `iterations` LM iterations, ONE cooperative
+ *   persistent kernel launch per iteration over all windows (capturable into a CUDA
+ *   graph): poses, disps updated in place, dx / dz written as hs2_ba does.
+ *   gram_split: pixel splits per depth frame of the Schur Gram (tuning knob, >= 1);
+ *   ctas_per_sm: CTAs per SM of the persistent grid (0 = as many as fit).
+ *   Each window's info [4] is as for hs2_ba.
+ */
+typedef struct hs2_ba_window {
+  float* poses;
+  int64_t num_poses;
+  float* disps;
+  int64_t num_disps;
+  int ht, wd;
+  const float* intrinsics;
+  const float* targets;
+  const float* weights;
+  const float* eta;
+  int64_t eta_rows;
+  const int64_t* ii;
+  const int64_t* jj;
+  int64_t num_edges;
+  int t0, t1;
+  float* dx;
+  float* dz;
+  int64_t dz_rows;
+  int32_t* info;
+} hs2_ba_window;
+int hs2_ba_batch_workspace_size(const hs2_ba_window* windows, int num_windows, size_t* bytes);
+int hs2_ba_batch_prepare(const hs2_ba_window* windows, int num_windows, int gram_split, int ctas_per_sm,
+                         void* workspace, size_t workspace_bytes, int* grid, hs2_stream_t stream);
+int hs2_ba_batch_run(void* workspace, int num_windows, int grid, int iterations, float lm, float ep,
+                     hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * ba_adjoint  (no operator of the reference: HI-SLAM2 differentiates its BA only
+ * through the pure-PyTorch path, hislam2/geom/ba.py + geom/chol.py:8-22)
+ *   Gradients of L(dx, dz) for ONE iteration of hs2_ba (motion_only = 0) with
+ *   respect to targets, weights [num_edges,2,ht,wd] and eta [eta_rows,ht,wd], at the
+ *   linearisation point poses/disps (those of the step, before it was applied):
+ *   implicit differentiation through the damped Schur solve, using the same
+ *   system build and Cholesky as the forward.  dx [t1-t0,6] is the step's output,
+ *   grad_dx [t1-t0,6] and grad_dz [dz_rows = M, ht*wd] are dL/ddx, dL/ddz; lam
+ *   [t1-t0,6] receives the adjoint pose solution.  All outputs are fully written.
+ *   info as for hs2_ba, plus HS2_DEV_LIMIT when a depth frame has more than 256
+ *   optimised rows or an edge pose more than 8 duplicate rows in one frame.
+ *   Workspace: hs2_ba_adjoint_workspace_size() bytes.
+ */
+int hs2_ba_adjoint_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd, int64_t num_edges, int t0,
+                                  int t1, size_t* bytes);
+int hs2_ba_adjoint(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht, int wd,
+                   const float* intrinsics, const float* targets, const float* weights, const float* eta,
+                   int64_t eta_rows, const int64_t* ii, const int64_t* jj, int64_t num_edges, int t0, int t1,
+                   float lm, float ep, const float* dx, const float* grad_dx, const float* grad_dz, int64_t dz_rows,
+                   float* grad_targets, float* grad_weights, float* grad_eta, float* lam, int32_t* info,
+                   void* workspace, size_t workspace_bytes, hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * corr_volume  (reference: hislam2/modules/corr.py:29-38,63-71 -- CorrBlock's
+ * all-pairs volume torch.matmul((f1/4)^T, f2/4) and its avg_pool2d pyramid, built by
+ * the caller in PyTorch; this entry point replaces that construction)
+ *   fmap1 [k1,channels,ht,wd], fmap2 [k2,channels,ht,wd] of `dtype` (HS2_F16 or
+ *   HS2_BF16), ii/jj [num_pairs] int64 (frame of fmap1 / fmap2 of each pair)
+ *   -> pyramid[l] [num_pairs, ht, wd, ht>>l, wd>>l] of `dtype` for l < levels (<= 4):
+ *   level 0 = sum_c (fmap1[ii,c]/4)(fmap2[jj,c]/4) accumulated in F32 on the tensor
+ *   cores, level l = 2x2 average of level l-1 (floor sizes), each level rounded to
+ *   `dtype` and pooled from the rounded level above (avg_pool2d's arithmetic).
+ *   precision HS2_CV_NATIVE contracts the 16-bit values as given; HS2_CV_E4M3
+ *   quantises each pixel's feature vector to FP8 e4m3 with its own scale
+ *   (max |f/4| / 448) and rescales the F32 sums.  channels must be 128, wd <= 96.
+ *   info: int32[1] on the device; info[0] |= HS2_DEV_BAD_INDEX for a pair whose frame
+ *   index is outside [0, k1) / [0, k2) (its outputs are left unwritten),
+ *   HS2_DEV_TIMEOUT if a bounded wait gave up.
+ *   Workspace: hs2_corr_volume_workspace_size() bytes (the packed operands).
+ */
+enum hs2_corr_precision { HS2_CV_NATIVE = 0, HS2_CV_E4M3 = 1 };
+int hs2_corr_volume_workspace_size(int64_t k1, int64_t k2, int channels, int ht, int wd, int dtype, int precision,
+                                   size_t* bytes);
+int hs2_corr_volume(const void* fmap1, int64_t k1, const void* fmap2, int64_t k2, int channels, int ht, int wd,
+                    int dtype, const int64_t* ii, const int64_t* jj, int64_t num_pairs, int precision, int levels,
+                    void* const* pyramid, int32_t* info, void* workspace, size_t workspace_bytes,
+                    hs2_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * corr_reproject_lookup  (reference: the caller side of the update step,
+ * hislam2/depth_video.py:170-178 reproject + hislam2/modules/corr.py:90-117
+ * AltCorrBlock, as factor_graph.py:194-200,253-260 chain them)
+ *   poses [num_poses,7], disps [num_disps,ht,wd], intrinsics [4] f32; fmap_levels[l]
+ *   [num_frames,channels,ht>>l,wd>>l] of `dtype` (level 0 = the features, l > 0 their
+ *   2x2 average pools); ii/jj [num_edges] int64
+ *   -> corr [num_edges, levels*(2r+1)^2, ht, wd] of `dtype`: the pixels of frame ii
+ *   projected into frame jj (Gij = Gj Gi^-1), scaled by 2^-l, and the bilinear
+ *   radius-r window of (f_ii/4).(f_jj,l/4) at every level -- one launch, no
+ *   coordinates or volume in memory.  coords1 [num_edges,ht,wd,2] f32 (optional,
+ *   NULL to skip) receives the level-0 coordinates.  info int32[1]:
+ *   HS2_DEV_BAD_INDEX for an edge outside the buffers (its outputs are zero).
+ */
+int hs2_corr_reproject_lookup(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps,
+                              const float* intrinsics, const void* const* fmap_levels, int levels, int dtype,
+                              int64_t num_frames, int channels, int ht, int wd, const int64_t* ii, const int64_t* jj,
+                              int64_t num_edges, int radius, void* corr, float* coords1, int32_t* info,
+                              hs2_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * altcorr_forward  (reference: src/droid.cpp:277-289, src/altcorr_kernel.cu:25-75,132-172)
@@ -265,14 +377,12 @@ int hs2_ba_set_schur_path(int path);
  * hs2_profile_enable(1) brackets every kernel launch of this library with CUDA
  * events on its stream; hs2_profile_report() waits for them and writes one line
  * per kernel, "<name> <launches> <total_ms>", into buf (returns the text length;
- * reset != 0 clears the record).  hs2_measure_simt_peaks() times FP32 and FP64
- * FMA chains on the current device (synchronous; allocates 8 bytes).
+ * reset != 0 clears the record).
  */
 void hs2_profile_enable(int on);
 /* Number of kernels this library has launched in this process. */
 long long hs2_launch_count(void);
 int hs2_profile_report(char* buf, size_t len, int reset);
-int hs2_measure_simt_peaks(double* fp32_tflops, double* fp64_tflops);
 
 #ifdef __cplusplus
 }

@@ -145,3 +145,67 @@ def test_geometry_ops_check_inputs_on_cpu():
         droid_backends.iproj(p, d, torch.zeros(4))
     with pytest.raises(RuntimeError, match="contiguous"):
         droid_backends.covis_distance(p, d.transpose(1, 2), torch.zeros(4), torch.ones(1, dtype=torch.long))
+
+
+def test_corr_volume_host_validation():
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    ok = lib.hs2_corr_volume_workspace_size(25, 25, 128, 43, 77, _lib.HS2_F16, _lib.HS2_CV_NATIVE, ctypes.byref(n))
+    assert ok == _lib.HS2_OK and n.value >= 50 * 3311 * 128 * 2
+    fp8 = ctypes.c_size_t(0)
+    assert lib.hs2_corr_volume_workspace_size(25, 25, 128, 43, 77, _lib.HS2_BF16, _lib.HS2_CV_E4M3,
+                                              ctypes.byref(fp8)) == _lib.HS2_OK
+    assert fp8.value < n.value                       # one byte per operand value plus the scales
+    assert lib.hs2_corr_volume_workspace_size(2, 2, 64, 43, 77, _lib.HS2_F16, 0, ctypes.byref(n)) == \
+        _lib.HS2_ERR_INVALID
+    assert b"128" in lib.hs2_last_error()
+    assert lib.hs2_corr_volume_workspace_size(2, 2, 128, 8, 100, _lib.HS2_F16, 0, ctypes.byref(n)) == \
+        _lib.HS2_ERR_INVALID
+    assert lib.hs2_corr_volume_workspace_size(2, 2, 128, 8, 64, _lib.HS2_F32, 0, ctypes.byref(n)) == \
+        _lib.HS2_ERR_DTYPE
+    assert lib.hs2_corr_volume_workspace_size(2, 2, 128, 8, 64, _lib.HS2_F16, 7, ctypes.byref(n)) == \
+        _lib.HS2_ERR_INVALID
+
+
+def test_ba_adjoint_and_batch_host_validation():
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.hs2_ba_adjoint_workspace_size(7, 7, 48, 64, 42, 2, 7, ctypes.byref(n)) == _lib.HS2_OK
+    base = ctypes.c_size_t(0)
+    lib.hs2_ba_workspace_size(7, 7, 48, 64, 42, 2, 7, 0, ctypes.byref(base))
+    assert n.value > base.value                      # the adjoint's per-pixel scratch on top
+    assert lib.hs2_ba_adjoint_workspace_size(7, 7, 48, 64, 42, 2, 8, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+    W = _lib.BaWindow
+    good = W(1, 10, 1, 10, 30, 40, 1, 1, 1, 1, 10, 1, 1, 40, 1, 10, 1, 1, 10, 1)
+    bad_t1 = W(1, 10, 1, 10, 30, 40, 1, 1, 1, 1, 10, 1, 1, 40, 1, 11, 1, 1, 10, 1)
+    too_many = W(1, 300, 1, 300, 30, 40, 1, 1, 1, 1, 300, 1, 1, 40, 0, 300, 1, 1, 300, 1)
+    null_dx = W(1, 10, 1, 10, 30, 40, 1, 1, 1, 1, 10, 1, 1, 40, 1, 10, 0, 1, 10, 1)
+    arr = (W * 2)(good, good)
+    assert lib.hs2_ba_batch_workspace_size(arr, 2, ctypes.byref(n)) == _lib.HS2_OK
+    one = ctypes.c_size_t(0)
+    assert lib.hs2_ba_batch_workspace_size((W * 1)(good), 1, ctypes.byref(one)) == _lib.HS2_OK
+    assert one.value < n.value
+    for bad, msg in ((bad_t1, b"t1"), (too_many, b"at most 256"), (null_dx, b"null")):
+        assert lib.hs2_ba_batch_workspace_size((W * 2)(good, bad), 2, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+        err = lib.hs2_last_error()
+        assert b"window 1" in err and msg in err, err
+    assert lib.hs2_ba_batch_workspace_size(arr, 0, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+
+
+def test_corr_reproject_lookup_host_validation():
+    lib = _lib.load()
+    ptrs = (ctypes.c_void_p * 4)(1, 1, 1, 1)
+    args = [1, 10, 1, 10, 1, ptrs, 4, _lib.HS2_F16, 10, 128, 43, 77, 1, 1, 20, 4, 1, None, 1, None]
+    bad_levels = list(args)
+    bad_levels[6] = 5
+    assert lib.hs2_corr_reproject_lookup(*bad_levels) == _lib.HS2_ERR_INVALID
+    tiny = list(args)
+    tiny[10], tiny[11] = 4, 4                        # 4 >> 3 == 0: no level-3 grid
+    assert lib.hs2_corr_reproject_lookup(*tiny) == _lib.HS2_ERR_INVALID
+    missing = list(args)
+    missing[5] = (ctypes.c_void_p * 4)(1, 1, 0, 1)
+    assert lib.hs2_corr_reproject_lookup(*missing) == _lib.HS2_ERR_INVALID
+    assert b"level 2" in lib.hs2_last_error()
+    empty = list(args)
+    empty[14] = 0
+    assert lib.hs2_corr_reproject_lookup(*empty) == _lib.HS2_OK

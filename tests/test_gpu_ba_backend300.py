@@ -1,0 +1,72 @@
+"""ba at the 300-keyframe backend size (300 kf, 43x77, 6000 edges, t0=10, lm=1e-5,
+ep=1e-2, 5% outliers) against the float64 oracle and the reference's own operator.
+
+Two Gauss-Newton iterations (one oracle iteration takes about 20 s on the host).
+Tolerances: poses, disparities, dx and dz within 1e-4 relative to their largest
+magnitude (the bar for the FP32 form), and the pose error against the FP64 oracle
+-- max |pose - pose_fp64| over all entries of the [300, 7] pose array, relative to
+max |pose_fp64| -- within 1e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import droid_backends
+import oracle
+from hislam2_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+ITERS = 2
+
+
+def rel(a, b):
+    a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else np.asarray(a, np.float64)
+    b = b.detach().double().cpu().numpy() if torch.is_tensor(b) else np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def backend300():
+    return synth.make_ba_problem("backend300", seed=0)
+
+
+@pytest.fixture(scope="module")
+def ours(backend300, cuda):
+    q = {k: (v.to(cuda) if torch.is_tensor(v) else v) for k, v in backend300.items()}
+    poses, disps = q["poses"].clone(), q["disps"].clone()
+    dx, dz, _ = droid_backends.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"],
+                                  q["jj"], q["t0"], q["t1"], ITERS, q["lm"], q["ep"], False)
+    torch.cuda.synchronize()
+    return poses, disps, dx, dz
+
+
+def test_backend300_matches_fp64_oracle(backend300, ours):
+    p = backend300
+    f = lambda k: p[k].double().numpy()  # noqa: E731
+    r = oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
+                     p["ii"].numpy(), p["jj"].numpy(), p["t0"], p["t1"], ITERS, p["lm"], p["ep"])
+    poses, disps, dx, dz = ours
+    pose_err = rel(poses, r.poses)
+    print("backend300, %d GN iterations: pose err %.2e, disp err %.2e, dx err %.2e, dz err %.2e"
+          % (ITERS, pose_err, rel(disps, r.disps), rel(dx, r.dx), rel(dz.reshape(r.dz.shape), r.dz)))
+    assert pose_err < 1e-5
+    assert rel(disps, r.disps) < 1e-4
+    assert rel(dx, r.dx) < 1e-4
+    assert rel(dz.reshape(r.dz.shape), r.dz) < 1e-4
+
+
+def test_backend300_matches_live_reference(backend300, ours, ref_ops, cuda):
+    if ref_ops is None:
+        pytest.skip("oracle/_ref not built")
+    q = {k: (v.to(cuda) if torch.is_tensor(v) else v) for k, v in backend300.items()}
+    poses, disps = q["poses"].clone(), q["disps"].clone()
+    dx, dz = ref_ops.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"], q["jj"],
+                        q["t0"], q["t1"], ITERS, q["lm"], q["ep"], False)[:2]
+    torch.cuda.synchronize()
+    po, do, xo, zo = ours
+    assert rel(po, poses) < 1e-5
+    assert rel(do, disps) < 1e-4
+    assert rel(xo, dx) < 1e-4
+    assert rel(zo.reshape(dz.shape), dz) < 1e-4
