@@ -192,11 +192,10 @@ ba_batch_kernel(const BatchHdr* __restrict__ hdr, const BatchWin* __restrict__ w
           unsigned i = 0;
           while (ld_acquire_gpu(c) < need) {
             if (++i > kBatchSpin || *(volatile int*)abort_flag) {
+              // only the launch-wide flag is raised here: the bodies of other CTAs read the
+              // windows' info words, which therefore must not change during the launch
               go = 0;
-              if (i > kBatchSpin) {
-                atomicOr(wins[lo].info, HS2_DEV_TIMEOUT);
-                atomicExch(abort_flag, 1);
-              }
+              if (i > kBatchSpin) atomicExch(abort_flag, 1);
               break;
             }
           }
@@ -213,6 +212,13 @@ ba_batch_kernel(const BatchHdr* __restrict__ hdr, const BatchWin* __restrict__ w
       red_release_add_gpu(done + s_w * kBatchPhases + s_ph, 1u);
     }
   }
+}
+
+// After a launch that gave up (a bounded wait ran out), every window's results are
+// incomplete: mark them all.
+__global__ void ba_batch_flag_kernel(const BatchWin* __restrict__ wins, int nwin, const int* __restrict__ abort_flag) {
+  if (*abort_flag == 0) return;
+  for (int k = threadIdx.x; k < nwin; k += blockDim.x) atomicOr(wins[k].info, HS2_DEV_TIMEOUT);
 }
 
 // ----------------------------------------------------------------- host ---
@@ -407,6 +413,8 @@ extern "C" int hs2_ba_batch_run(void* workspace, int num_windows, int grid, int 
     HS2_PROF("ba_batch", s);
     HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_batch_kernel, dim3(grid), dim3(kBatchThreads), args, 0, s));
     HS2_LAUNCH_CHECK("ba_batch_kernel");
+    ba_batch_flag_kernel<<<1, 64, 0, s>>>(dw, nwin, abort_flag);
+    HS2_LAUNCH_CHECK("ba_batch_flag_kernel");
   }
   return HS2_OK;
 }
