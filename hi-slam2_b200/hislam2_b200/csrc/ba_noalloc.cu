@@ -1,12 +1,11 @@
 // hs2_ba_noalloc: bundle adjustment that allocates nothing.
 //
 // Some callers cannot allocate device memory at the moment they run a BA step:
-// a tracker thread that is being recorded into a CUDA graph (cudaMalloc is not
-// allowed while a stream is capturing), a real-time process that fixes its GPU
-// memory budget at start-up, or a host in another language that has no caching
-// allocator and cannot afford the device-wide synchronisation of cudaMalloc /
-// cudaFree in its tracking loop.  For them this entry point takes its scratch
-// from one static device array of this file instead of a caller workspace.
+// a real-time process that fixes its GPU memory budget at start-up, or a host in
+// another language that has no caching allocator and cannot afford the
+// device-wide synchronisation of cudaMalloc / cudaFree in its tracking loop.  For
+// them this entry point takes its scratch from one static device array of this file
+// instead of a caller workspace.
 //
 // The array is sized for a frontend window (kNoAllocScratchBytes = 64 MiB,
 // enough for e.g. 25 keyframes and ~300 edges on a 43x77 grid); every GPU that

@@ -231,7 +231,7 @@ int hs2_altcorr_backward(const void* fmap1, const void* fmap2, int dtype, int b,
  *   iterations whose Cholesky factorisation failed (their dx is 0, as in the
  *   reference), [3] reserved.  When info[0] != 0 nothing was modified.
  *   workspace: hs2_ba_workspace_size() bytes, 256-byte aligned.
- *   No host synchronisation; safe to capture in a CUDA graph.
+ *   No host synchronisation.
  */
 int hs2_ba_workspace_size(int64_t num_poses, int64_t num_disps, int ht, int wd, int64_t num_edges,
                           int t0, int t1, int motion_only, size_t* bytes);
@@ -267,9 +267,10 @@ int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int64_t num_di
              size_t workspace_bytes, hs2_stream_t stream);
 
 /* ba without allocation.  No counterpart in the reference: this entry point is for
- * callers that cannot allocate device memory when they run a BA step (a stream
- * being captured into a CUDA graph, a process with a GPU memory budget fixed at
- * start-up, a foreign-language host without a caching allocator).  Same arguments
+ * callers that cannot allocate device memory when they run a BA step (a process with
+ * a GPU memory budget fixed at start-up, a foreign-language host without a caching
+ * allocator, for which cudaMalloc / cudaFree in the tracking loop would stall the
+ * device).  Same arguments
  * and results as hs2_ba, minus the workspace: the scratch is a static device array
  * of 64 MiB inside the library, held by every GPU that loads it until exit.
  * Problems whose hs2_ba_workspace_size() exceeds 64 MiB are rejected with

@@ -1,9 +1,9 @@
 """The allocation-free BA entry point (hs2_ba_noalloc) against the regular one.
 
 hs2_ba_noalloc serves callers that cannot allocate device memory when they run a
-BA step -- a stream being captured into a CUDA graph, a process whose GPU memory
-budget is fixed at start-up, or a host in another language without a caching
-allocator.  It takes its scratch from a 64 MiB static device array inside the
+BA step -- a process whose GPU memory budget is fixed at start-up, or a host in
+another language without a caching allocator, for which cudaMalloc / cudaFree in
+its loop would stall the device.  It takes its scratch from a 64 MiB static device array inside the
 library instead of a caller workspace.  This test calls it through the C ABI on
 two problems in a row (so the second call runs on the scratch the first one left
 behind) and compares poses, disparities, dx and dz with droid_backends.ba, within
