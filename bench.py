@@ -662,15 +662,20 @@ def reference_corr_lookup(ref, args, dev):
     """The reference's corr_index_forward on the same 4-level radius-4 frontend lookup as ours."""
     pyr, crds, r, bytes_per = frontend_lookup_inputs(dev)
 
+    E = pyr[0].shape[0]
+    halves = [(0, E // 2), (E // 2, E)]   # its 32-bit accessors take < 2^31 elements per volume
+
     def step():
         for lvl in range(4):
-            ref.corr_index_forward(pyr[lvl], crds[lvl], r)
+            for a, b in halves:
+                ref.corr_index_forward(pyr[lvl][a:b], crds[lvl][a:b], r)
 
     ms = device_time(step, args.steps)
     del pyr
     torch.cuda.empty_cache()
     return {"value": round(bytes_per / (ms / 1e3) / 1e9, 2), "unit": "GB/s", "ms_per_lookup": round(ms, 4),
-            "config": "258 edges (frontend window), 43x77, 4 levels, radius 4, fp16 volumes"}
+            "config": "258 edges (frontend window) in two calls of 129 (the op's 32-bit accessors take < 2^31 "
+                      "elements per volume), 43x77, 4 levels, radius 4, fp16 volumes"}
 
 
 # ------------------------------------------------------------ profiler cases
@@ -714,7 +719,16 @@ def profile_adjoint(args, dev):
                         torch.ones_like(dz))
 
 
-PROFILE_CASES = {"ba": profile_ba, "volume": profile_volume, "adjoint": profile_adjoint}
+def profile_batch(args, dev):
+    """One batched LM iteration over the first --profile-edges windows of the batching workload."""
+    from hislam2_b200 import backends, synth
+    ws = [{k: (v.to(dev) if torch.is_tensor(v) else v) for k, v in w.items()}
+          for w in synth.make_batch_problems(num_windows=min(64, args.profile_edges), seed=0)]
+    plan = backends.BABatch(ws, 1e-4, 0.1)
+    plan.run(args.profile_iters)
+
+
+PROFILE_CASES = {"ba": profile_ba, "volume": profile_volume, "adjoint": profile_adjoint, "batch": profile_batch}
 
 
 def main():

@@ -7,8 +7,10 @@ the Eigen facilities replaced by the dense stand-in in oracle/eigen_standin) on 
 GPU, on the seeded tiny6 / tiny7 problems.  The reference computes in float32 on
 the GPU and solves the reduced system in float64; the oracle is float64
 throughout.  Tolerances (relative to the largest magnitude of each output):
-poses, disparities, dx, dz and the geometry outputs 1e-4 (the bar for the FP32
-form); counts (depth_filter) must agree on all but boundary pixels.
+poses, disparities and the geometry outputs 1e-4 (the bar for the FP32 form); dx and
+dz, which the fixtures record for the LAST of three iterations (converged updates
+whose relative rounding is larger), 1e-3; counts (depth_filter) must agree on all
+but boundary pixels.
 """
 
 import glob
@@ -44,12 +46,12 @@ def test_ba_oracle_matches_reference(path):
                      motion_only)
     assert rel(r.poses, d["out_poses"]) < 1e-4
     assert rel(r.disps, d["out_disps"]) < 1e-4
-    assert rel(r.dx, d["dx"]) < 1e-4
+    assert rel(r.dx, d["dx"]) < 1e-3
     if motion_only:
         assert "dz" not in d.files
         np.testing.assert_array_equal(r.disps, d["disps"])
     else:
-        assert rel(r.dz.reshape(d["dz"].shape), d["dz"]) < 1e-4
+        assert rel(r.dz.reshape(d["dz"].shape), d["dz"]) < 1e-3
 
 
 def test_ba_reference_leaves_frames_outside_the_window_and_graph_alone():

@@ -2,10 +2,11 @@
 ep=1e-2, 5% outliers) against the float64 oracle and the reference's own operator.
 
 Two Gauss-Newton iterations (one oracle iteration takes about 20 s on the host).
-Tolerances: poses, disparities, dx and dz within 1e-4 relative to their largest
-magnitude (the bar for the FP32 form), and the pose error against the FP64 oracle
--- max |pose - pose_fp64| over all entries of the [300, 7] pose array, relative to
-max |pose_fp64| -- within 1e-5.
+Tolerances: disparities after two iterations and dx / dz of the first iteration within
+1e-4 relative to their largest magnitude (the bar for the FP32 form), and the pose
+error against the FP64 oracle -- max |pose - pose_fp64| over all entries of the
+[300, 7] pose array, relative to max |pose_fp64| -- within 1e-5.  (dx of the second,
+nearly converged iteration is not a meaningful relative comparison.)
 """
 
 import numpy as np
@@ -32,13 +33,20 @@ def backend300():
     return synth.make_ba_problem("backend300", seed=0)
 
 
-@pytest.fixture(scope="module")
-def ours(backend300, cuda):
-    q = {k: (v.to(cuda) if torch.is_tensor(v) else v) for k, v in backend300.items()}
+def run(p, dev, iters):
+    q = {k: (v.to(dev) if torch.is_tensor(v) else v) for k, v in p.items()}
     poses, disps = q["poses"].clone(), q["disps"].clone()
     dx, dz, _ = droid_backends.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"],
-                                  q["jj"], q["t0"], q["t1"], ITERS, q["lm"], q["ep"], False)
+                                  q["jj"], q["t0"], q["t1"], iters, q["lm"], q["ep"], False)
     torch.cuda.synchronize()
+    return poses, disps, dx, dz
+
+
+@pytest.fixture(scope="module")
+def ours(backend300, cuda):
+    """(poses, disps) after ITERS iterations and (dx, dz) of a single first iteration."""
+    poses, disps, _, _ = run(backend300, cuda, ITERS)
+    _, _, dx, dz = run(backend300, cuda, 1)
     return poses, disps, dx, dz
 
 
@@ -46,26 +54,33 @@ def test_backend300_matches_fp64_oracle(backend300, ours):
     p = backend300
     f = lambda k: p[k].double().numpy()  # noqa: E731
     r = oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
-                     p["ii"].numpy(), p["jj"].numpy(), p["t0"], p["t1"], ITERS, p["lm"], p["ep"])
+                     p["ii"].numpy(), p["jj"].numpy(), p["t0"], p["t1"], ITERS, p["lm"], p["ep"], trace=True)
     poses, disps, dx, dz = ours
+    rdx, rdz = r.traces[0]["dx"], r.traces[0]["dz"]
     pose_err = rel(poses, r.poses)
-    print("backend300, %d GN iterations: pose err %.2e, disp err %.2e, dx err %.2e, dz err %.2e"
-          % (ITERS, pose_err, rel(disps, r.disps), rel(dx, r.dx), rel(dz.reshape(r.dz.shape), r.dz)))
+    print("backend300, %d GN iterations: pose err %.2e, disp err %.2e; first iteration dx err %.2e, dz err %.2e"
+          % (ITERS, pose_err, rel(disps, r.disps), rel(dx, rdx), rel(dz.reshape(rdz.shape), rdz)))
     assert pose_err < 1e-5
     assert rel(disps, r.disps) < 1e-4
-    assert rel(dx, r.dx) < 1e-4
-    assert rel(dz.reshape(r.dz.shape), r.dz) < 1e-4
+    assert rel(dx, rdx) < 1e-4
+    assert rel(dz.reshape(rdz.shape), rdz) < 1e-4
 
 
 def test_backend300_matches_live_reference(backend300, ours, ref_ops, cuda):
     if ref_ops is None:
         pytest.skip("oracle/_ref not built")
     q = {k: (v.to(cuda) if torch.is_tensor(v) else v) for k, v in backend300.items()}
-    poses, disps = q["poses"].clone(), q["disps"].clone()
-    dx, dz = ref_ops.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"], q["jj"],
-                        q["t0"], q["t1"], ITERS, q["lm"], q["ep"], False)[:2]
-    torch.cuda.synchronize()
+
+    def ref(iters):
+        poses, disps = q["poses"].clone(), q["disps"].clone()
+        dx, dz = ref_ops.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"], q["jj"],
+                            q["t0"], q["t1"], iters, q["lm"], q["ep"], False)[:2]
+        torch.cuda.synchronize()
+        return poses, disps, dx, dz
+
     po, do, xo, zo = ours
+    poses, disps, _, _ = ref(ITERS)
+    _, _, dx, dz = ref(1)
     assert rel(po, poses) < 1e-5
     assert rel(do, disps) < 1e-4
     assert rel(xo, dx) < 1e-4

@@ -2,10 +2,11 @@
 against the single-window operator (droid_backends.ba) on every window, and against
 the float64 oracle on the small ones.
 
-Tolerance: 1e-4 relative to the largest magnitude for poses, disparities, dx and dz
-(the bar of the FP32 form; the batch runs the same linearisation, the SIMT Gram in
-FP32 and a single-CTA FP64 Cholesky, so it agrees with the single-window path to
-FP32 rounding).
+Tolerance: 1e-4 relative to the largest magnitude for poses and disparities after
+several iterations and for dx and dz of a first iteration (the bar of the FP32 form;
+the batch runs the same linearisation, the SIMT Gram in FP32 and a single-CTA FP64
+Cholesky, so it agrees with the single-window path to FP32 rounding).  dx / dz of the
+last of several iterations are not compared: converged, they are rounding noise.
 """
 
 import numpy as np
@@ -47,19 +48,25 @@ def mixed_windows():
     return ws + synth.make_batch_problems(num_windows=5, seed=7)
 
 
+def run_batch(ws, dev, iters, lm, ep, **kw):
+    dev_ws = [on(dict(w, lm=lm, ep=ep), dev) for w in ws]
+    plan = backends.BABatch(dev_ws, lm, ep, **kw)
+    plan.run(iters)
+    torch.cuda.synchronize()
+    return dev_ws, plan.results()
+
+
 @pytest.mark.parametrize("gram_split,ctas", [(1, 0), (4, 1), (8, 2)])
 def test_batch_matches_single_window_operator(cuda, gram_split, ctas):
     ws = mixed_windows()
-    lm, ep, iters = 1e-4, 0.1, 3
-    dev_ws = [on(dict(w, lm=lm, ep=ep), cuda) for w in ws]
-    plan = backends.BABatch(dev_ws, lm, ep, gram_split=gram_split, ctas_per_sm=ctas)
-    plan.run(iters)
-    torch.cuda.synchronize()
-    res = plan.results()
+    lm, ep = 1e-4, 0.1
+    dev_ws, _ = run_batch(ws, cuda, 3, lm, ep, gram_split=gram_split, ctas_per_sm=ctas)
+    one_ws, res = run_batch(ws, cuda, 1, lm, ep, gram_split=gram_split, ctas_per_sm=ctas)
     for k, w in enumerate(ws):
-        po, do, xo, zo = single(dict(w, lm=lm, ep=ep), cuda, iters)
+        po, do, _, _ = single(dict(w, lm=lm, ep=ep), cuda, 3)
         assert rel(dev_ws[k]["poses"], po) < RTOL, k
         assert rel(dev_ws[k]["disps"], do) < RTOL, k
+        _, _, xo, zo = single(dict(w, lm=lm, ep=ep), cuda, 1)
         assert rel(res[k][0], xo) < RTOL, k
         assert rel(res[k][1], zo) < RTOL, k
 
@@ -67,31 +74,30 @@ def test_batch_matches_single_window_operator(cuda, gram_split, ctas):
 def test_batch_small_windows_match_oracle(cuda):
     ws = mixed_windows()[:3]
     lm, ep, iters = 1e-4, 0.1, 2
-    dev_ws = [on(w, cuda) for w in ws]
-    plan = backends.BABatch(dev_ws, lm, ep)
-    plan.run(iters)
-    res = plan.results()
+    dev_ws, _ = run_batch(ws, cuda, iters, lm, ep)
+    _, res = run_batch(ws, cuda, 1, lm, ep)
     for k, w in enumerate(ws):
         f = lambda n: w[n].double().numpy()  # noqa: E731
         r = oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
-                         w["ii"].numpy(), w["jj"].numpy(), w["t0"], w["t1"], iters, lm, ep)
+                         w["ii"].numpy(), w["jj"].numpy(), w["t0"], w["t1"], iters, lm, ep, trace=True)
         assert rel(dev_ws[k]["poses"], r.poses) < RTOL
         assert rel(dev_ws[k]["disps"], r.disps) < RTOL
-        assert rel(res[k][0], r.dx) < RTOL
+        assert rel(res[k][0], r.traces[0]["dx"]) < RTOL
+        assert rel(res[k][1], r.traces[0]["dz"].reshape(res[k][1].shape)) < RTOL
 
 
 def test_batch_64_uneven_windows(cuda):
     """The batching configuration: 64 windows, keyframes 8..40, edges 20..500, 43x77 or 30x40."""
     ws = synth.make_batch_problems(num_windows=64, seed=0)
     lm, ep, iters = 1e-4, 0.1, 4
-    dev_ws = [on(w, cuda) for w in ws]
-    plan = backends.BABatch(dev_ws, lm, ep)
-    plan.run(iters)
-    res = plan.results()
+    dev_ws, _ = run_batch(ws, cuda, iters, lm, ep)
+    _, res = run_batch(ws, cuda, 1, lm, ep)
     worst = 0.0
     for k in range(0, 64, 7):
-        po, do, xo, zo = single(ws[k], cuda, iters)
-        worst = max(worst, rel(dev_ws[k]["poses"], po), rel(dev_ws[k]["disps"], do), rel(res[k][0], xo))
+        po, do, _, _ = single(ws[k], cuda, iters)
+        _, _, xo, zo = single(ws[k], cuda, 1)
+        worst = max(worst, rel(dev_ws[k]["poses"], po), rel(dev_ws[k]["disps"], do), rel(res[k][0], xo),
+                    rel(res[k][1], zo))
     print("64 windows: worst relative difference to the single-window operator %.2e" % worst)
     assert worst < RTOL
 

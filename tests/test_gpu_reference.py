@@ -53,11 +53,11 @@ def test_ba_matches_reference_fixture(cuda, path):
                                   float(d["ep"]), bool(d["motion_only"]))
     assert rel(poses, d["out_poses"]) < RTOL
     assert rel(disps, d["out_disps"]) < RTOL
-    assert rel(dx, d["dx"]) < RTOL
+    assert rel(dx, d["dx"]) < 1e-3            # the last of three iterations: a converged update
     if bool(d["motion_only"]):
         assert dz is None
     else:
-        assert rel(dz.reshape(d["dz"].shape), d["dz"]) < RTOL
+        assert rel(dz.reshape(d["dz"].shape), d["dz"]) < 1e-3
 
 
 def test_pgba_matches_reference_fixture(cuda):
@@ -136,11 +136,14 @@ def run_both(fn_ours, fn_ref, p, dev, iters, motion_only=False):
 @pytest.mark.parametrize("case", sorted(LIVE))
 @pytest.mark.parametrize("motion_only", [False, True], ids=["full", "motion_only"])
 def test_ba_matches_live_reference(cuda, ref_ops, case, motion_only):
+    """Poses and disparities after the workload's iterations; dx and dz of a first
+    iteration (those of a later, converged iteration are rounding noise)."""
     _need(ref_ops)
     p = LIVE[case]()
-    (po, do, xo, zo), (pr, dr, xr, zr) = run_both(droid_backends.ba, ref_ops.ba, p, cuda, p["iters"], motion_only)
+    (po, do, _, _), (pr, dr, _, _) = run_both(droid_backends.ba, ref_ops.ba, p, cuda, p["iters"], motion_only)
     assert rel(po, pr) < RTOL
     assert rel(do, dr) < RTOL
+    (_, _, xo, zo), (_, _, xr, zr) = run_both(droid_backends.ba, ref_ops.ba, p, cuda, 1, motion_only)
     assert rel(xo, xr) < RTOL
     if not motion_only:
         assert rel(zo.reshape(zr.shape), zr) < RTOL
@@ -172,6 +175,10 @@ def frontend_pyramid(dev, dtype):
     return pyr, coords, c["radius"]
 
 
+def halves(n):
+    return [(0, n // 2), (n // 2, n)]
+
+
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16], ids=["f32", "f16"])
 def test_corr_lookup_frontend_window_matches_live_reference(cuda, ref_ops, dtype):
     """258 edges, 43x77, radius 4, all four pyramid levels (coords / 2^level)."""
@@ -182,14 +189,16 @@ def test_corr_lookup_frontend_window_matches_live_reference(cuda, ref_ops, dtype
     for lvl, vol in enumerate(pyr):
         crd = (coords / 2 ** lvl).contiguous()
         ours, = droid_backends.corr_index_forward(vol, crd, r)
-        ref, = ref_ops.corr_index_forward(vol, crd, r)
+        # the reference op indexes with 32-bit accessors: level 0 of 258 edges (2.8e9
+        # elements) is fed to it in two halves
+        ref = torch.cat([ref_ops.corr_index_forward(vol[a:b], crd[a:b], r)[0] for a, b in halves(vol.shape[0])])
         assert ours.shape == ref.shape == (vol.shape[0], (2 * r + 1) ** 2) + vol.shape[1:3]
         errs.append(rel(ours, ref))
         g = torch.randn(ours.shape, device=cuda, generator=torch.Generator(cuda).manual_seed(lvl)).to(dtype)
         vg_ours, = droid_backends.corr_index_backward(vol, crd, g, r)
-        vg_ref, = ref_ops.corr_index_backward(vol, crd, g, r)
-        errs.append(rel(vg_ours, vg_ref))
-        del vg_ours, vg_ref
+        errs.append(max(rel(vg_ours[a:b], ref_ops.corr_index_backward(vol[a:b], crd[a:b], g[a:b], r)[0])
+                        for a, b in halves(vol.shape[0])))
+        del vg_ours
     print("corr lookup %s: max relative difference to the reference per level (fwd, bwd): %s"
           % (dtype, ["%.2e" % e for e in errs]))
     assert max(errs) < tol, errs
