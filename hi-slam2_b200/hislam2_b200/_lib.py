@@ -79,6 +79,7 @@ SIGNATURES.update({
     "hs2_ba_batch_workspace_size": [ctypes.POINTER(BaWindow), _i32, ctypes.POINTER(_sz)],
     "hs2_ba_batch_prepare": [ctypes.POINTER(BaWindow), _i32, _i32, _i32, _p, _sz, ctypes.POINTER(_i32), _p],
     "hs2_ba_batch_run": [_p, _i32, _i32, _i32, _f32, _f32, _p],
+    "hs2_ba_batch_set_wait_test": [ctypes.c_uint, _i32],
 })
 
 _lib = None

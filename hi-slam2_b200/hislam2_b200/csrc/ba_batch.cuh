@@ -12,7 +12,8 @@
 //   2  assembly (256 edge threads per unit) and the SIMT Schur Gram, one unit per
 //      (depth frame, pixel split) (ba_schur body);
 //   3  the damped FP64 Cholesky solve of the window's reduced system, one unit
-//      (single CTA: the systems are at most 6 * kBatchMaxPoses wide);
+//      (single CTA: 32-column panels in shared memory for systems up to 256 wide,
+//      column by column in global memory above that, up to 6 * kBatchMaxPoses);
 //   4  back-substitution per (depth frame, 1024 pixels) and the pose retraction.
 // A unit of phase k > 0 waits (acquire, bounded) until the window's phase k-1
 // counter reaches its unit count; units count themselves done with a release add.
@@ -27,6 +28,12 @@ constexpr int kBatchThreads = 256;
 constexpr int kBatchPhases = 5;
 constexpr int kBatchMaxPoses = 256;     // 6 * 256 = 1536-wide reduced systems at most
 constexpr unsigned kBatchSpin = 1u << 24;
+
+// Test hooks for the bounded waits (hs2_ba_batch_set_wait_test): the number of polls
+// a dependency wait makes before it gives up, and a switch that adds one to every
+// count a wait needs, so that no wait can be satisfied and each one runs out.
+__device__ unsigned g_batch_spin = kBatchSpin;
+__device__ unsigned g_batch_unsatisfiable = 0;
 
 struct BatchWin {
   float* poses;
@@ -120,7 +127,138 @@ __device__ void batch_cholesky_solve(int n, float lm, float ep, BaPtrs w, float*
   }
 }
 
-__device__ void batch_unit(const BatchWin& W, int ph, int idx, float lm, float ep) {
+// Blocked form of the same factorisation and solve for systems of at most
+// kBatchPanelRows unknowns: 32-column panels are factored in shared memory (pv:
+// kBatchPanelRows x 33 doubles of dynamic shared memory), the trailing matrix is
+// updated with 32-long dot products against the panel, and the two triangular
+// solves go block by block (diagonal block in shared memory, one warp eliminating
+// its 32 unknowns, all threads applying the off-diagonal blocks).  Same results as
+// batch_cholesky_solve up to rounding; same failure rule.
+constexpr int kBatchPanelRows = 256;
+constexpr int kBatchPanelLd = 33;
+constexpr size_t kBatchDynSmem = sizeof(double) * kBatchPanelRows * kBatchPanelLd;
+
+__device__ void batch_cholesky_blocked(int n, float lm, float ep, BaPtrs w, float* __restrict__ dx,
+                                       int32_t* __restrict__ info, double* __restrict__ pv) {
+  double* A = w.A;
+  double* y = w.b;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kBatchThreads / 32;
+  __shared__ int failed;
+  __shared__ double red[NW][32];
+  if (tid == 0) failed = 0;
+  for (int i = tid; i < n; i += kBatchThreads) {
+    const double d = A[(int64_t)i * n + i];
+    A[(int64_t)i * n + i] = d + (ep + lm * d);
+  }
+  __syncthreads();
+  for (int kb = 0; kb < n; kb += 32) {
+    const int nc = min(32, n - kb), rows = n - kb;
+    for (int i = warp; i < rows; i += NW)
+      for (int c = lane; c < nc; c += 32) pv[i * kBatchPanelLd + c] = c <= i ? A[(int64_t)(kb + i) * n + kb + c] : 0.0;
+    __syncthreads();
+    for (int c = 0; c < nc; ++c) {
+      if (tid == 0) {
+        const double d = pv[c * kBatchPanelLd + c];
+        if (!(d > 0.0)) failed = 1;
+        else pv[c * kBatchPanelLd + c] = sqrt(d);
+      }
+      __syncthreads();
+      if (failed) break;
+      const double inv = 1.0 / pv[c * kBatchPanelLd + c];
+      for (int i = c + 1 + tid; i < rows; i += kBatchThreads) pv[i * kBatchPanelLd + c] *= inv;
+      __syncthreads();
+      // rank-1 update of the panel's remaining columns (c2 <= i)
+      for (int i = c + 1 + warp; i < rows; i += NW) {
+        const double lic = pv[i * kBatchPanelLd + c];
+        for (int c2 = c + 1 + lane; c2 < nc && c2 <= i; c2 += 32)
+          pv[i * kBatchPanelLd + c2] -= lic * pv[c2 * kBatchPanelLd + c];
+      }
+      __syncthreads();
+    }
+    if (failed) break;
+    for (int i = warp; i < rows; i += NW)
+      for (int c = lane; c < nc; c += 32)
+        if (c <= i) A[(int64_t)(kb + i) * n + kb + c] = pv[i * kBatchPanelLd + c];
+    // trailing update A[i][j] -= L[i, panel] . L[j, panel] for kb + nc <= j <= i
+    for (int i = nc + warp; i < rows; i += NW) {
+      const double* li = pv + i * kBatchPanelLd;
+      for (int j = nc + lane; j <= i; j += 32) {
+        const double* lj = pv + j * kBatchPanelLd;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int c = 0; c < nc; ++c) acc = fma(li[c], lj[c], acc);
+        A[(int64_t)(kb + i) * n + kb + j] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    for (int i = tid; i < n; i += kBatchThreads) {
+      w.x[i] = 0.0;
+      dx[i] = 0.f;
+    }
+    if (tid == 0) atomicAdd(&info[2], 1);
+    return;
+  }
+  // forward L y = b, block by block (y in place in w.b)
+  for (int kb = 0; kb < n; kb += 32) {
+    const int nc = min(32, n - kb);
+    for (int i = warp; i < nc; i += NW)
+      for (int c = lane; c <= i; c += 32) pv[i * kBatchPanelLd + c] = A[(int64_t)(kb + i) * n + kb + c];
+    __syncthreads();
+    if (warp == 0) {
+      double yc = lane < nc ? y[kb + lane] : 0.0;
+      for (int k = 0; k < nc; ++k) {
+        if (lane == k) yc /= pv[k * kBatchPanelLd + k];
+        const double yk = __shfl_sync(0xffffffffu, yc, k);
+        if (lane > k && lane < nc) yc -= pv[lane * kBatchPanelLd + k] * yk;
+      }
+      if (lane < nc) y[kb + lane] = yc;
+    }
+    __syncthreads();
+    for (int i = kb + nc + tid; i < n; i += kBatchThreads) {
+      double acc = 0.0;
+      for (int c = 0; c < nc; ++c) acc = fma(A[(int64_t)i * n + kb + c], y[kb + c], acc);
+      y[i] -= acc;
+    }
+    __syncthreads();
+  }
+  // backward L^T x = y, last block first
+  const int nblk = (n + 31) / 32;
+  for (int bk = nblk - 1; bk >= 0; --bk) {
+    const int kb = bk * 32, nc = min(32, n - kb);
+    // y[kb + c] -= sum_{i >= kb + nc} L[i][kb + c] x[i]
+    double part = 0.0;
+    if (lane < nc)
+      for (int i = kb + nc + warp; i < n; i += NW) part = fma(A[(int64_t)i * n + kb + lane], y[i], part);
+    red[warp][lane] = part;
+    for (int i = warp; i < nc; i += NW)
+      for (int c = lane; c <= i; c += 32) pv[i * kBatchPanelLd + c] = A[(int64_t)(kb + i) * n + kb + c];
+    __syncthreads();
+    if (warp == 0) {
+      double yc = 0.0;
+      if (lane < nc) {
+        double t = 0.0;
+        for (int k = 0; k < NW; ++k) t += red[k][lane];
+        yc = y[kb + lane] - t;
+      }
+      for (int k = nc - 1; k >= 0; --k) {
+        if (lane == k) yc /= pv[k * kBatchPanelLd + k];
+        const double xk = __shfl_sync(0xffffffffu, yc, k);
+        if (lane < k) yc -= pv[k * kBatchPanelLd + lane] * xk;
+      }
+      if (lane < nc) y[kb + lane] = yc;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < n; i += kBatchThreads) {
+    w.x[i] = y[i];
+    dx[i] = (float)y[i];
+  }
+}
+
+__device__ void batch_unit(const BatchWin& W, int ph, int idx, float lm, float ep, double* pv) {
   const int tid = threadIdx.x;
   const BaPtrs& w = W.w;
   const int n = 6 * W.P;
@@ -148,7 +286,10 @@ __device__ void batch_unit(const BatchWin& W, int ph, int idx, float lm, float e
       }
       break;
     case 3:
-      if (W.info[0] == 0 && n > 0) batch_cholesky_solve(n, lm, ep, w, W.dx, W.info);
+      if (W.info[0] == 0 && n > 0) {
+        if (n <= kBatchPanelRows) batch_cholesky_blocked(n, lm, ep, w, W.dx, W.info, pv);
+        else batch_cholesky_solve(n, lm, ep, w, W.dx, W.info);
+      }
       break;
     default:
       if (idx < W.nback) {
@@ -166,6 +307,7 @@ ba_batch_kernel(const BatchHdr* __restrict__ hdr, const BatchWin* __restrict__ w
                 unsigned* __restrict__ done, unsigned* __restrict__ next, int* __restrict__ abort_flag, float lm,
                 float ep) {
   __shared__ int s_u, s_ph, s_w, s_idx, s_go;
+  extern __shared__ double batch_dyn[];       // the blocked Cholesky's panel
   const int nwin = hdr->nwin, total = hdr->total;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -187,15 +329,16 @@ ba_batch_kernel(const BatchHdr* __restrict__ hdr, const BatchWin* __restrict__ w
         s_idx = local - pre[lo];
         int go = 1;
         if (ph > 0) {
-          const unsigned need = (unsigned)wins[lo].units[ph - 1];
+          const unsigned need = (unsigned)wins[lo].units[ph - 1] + g_batch_unsatisfiable;
+          const unsigned limit = g_batch_spin;
           const unsigned* c = done + lo * kBatchPhases + ph - 1;
           unsigned i = 0;
           while (ld_acquire_gpu(c) < need) {
-            if (++i > kBatchSpin || *(volatile int*)abort_flag) {
+            if (++i > limit || *(volatile int*)abort_flag) {
               // only the launch-wide flag is raised here: the bodies of other CTAs read the
               // windows' info words, which therefore must not change during the launch
               go = 0;
-              if (i > kBatchSpin) atomicExch(abort_flag, 1);
+              if (i > limit) atomicExch(abort_flag, 1);
               break;
             }
           }
@@ -205,7 +348,7 @@ ba_batch_kernel(const BatchHdr* __restrict__ hdr, const BatchWin* __restrict__ w
     }
     __syncthreads();
     if (s_u >= total) break;
-    if (s_go) batch_unit(wins[s_w], s_ph, s_idx, lm, ep);
+    if (s_go) batch_unit(wins[s_w], s_ph, s_idx, lm, ep, batch_dyn);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
@@ -354,7 +497,8 @@ extern "C" int hs2_ba_batch_prepare(const hs2_ba_window* windows, int num_window
   int dev = 0, sms = 0, occ = 0;
   HS2_CUDA(cudaGetDevice(&dev));
   HS2_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  HS2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ba_batch_kernel, kBatchThreads, 0));
+  HS2_CUDA(cudaFuncSetAttribute(ba_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchDynSmem));
+  HS2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ba_batch_kernel, kBatchThreads, kBatchDynSmem));
   if (occ < 1) {
     set_error("ba_batch_prepare: the batched kernel does not fit on an SM");
     return HS2_ERR_CUDA;
@@ -411,10 +555,20 @@ extern "C" int hs2_ba_batch_run(void* workspace, int num_windows, int grid, int 
     HS2_CUDA(cudaMemsetAsync(done, 0, ctl_bytes, s));
     void* args[] = {&dh, &dw, &dp, &done, &next, &abort_flag, &lm, &ep};
     HS2_PROF("ba_batch", s);
-    HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_batch_kernel, dim3(grid), dim3(kBatchThreads), args, 0, s));
+    HS2_CUDA(cudaLaunchCooperativeKernel((const void*)ba_batch_kernel, dim3(grid), dim3(kBatchThreads), args,
+                                         kBatchDynSmem, s));
     HS2_LAUNCH_CHECK("ba_batch_kernel");
     ba_batch_flag_kernel<<<1, 64, 0, s>>>(dw, nwin, abort_flag);
     HS2_LAUNCH_CHECK("ba_batch_flag_kernel");
   }
+  return HS2_OK;
+}
+
+extern "C" int hs2_ba_batch_set_wait_test(unsigned spin_limit, int unsatisfiable) {
+  using namespace hs2;
+  const unsigned spin = spin_limit == 0 ? kBatchSpin : spin_limit;
+  const unsigned add = unsatisfiable ? 1u : 0u;
+  HS2_CUDA(cudaMemcpyToSymbol(g_batch_spin, &spin, sizeof(spin)));
+  HS2_CUDA(cudaMemcpyToSymbol(g_batch_unsatisfiable, &add, sizeof(add)));
   return HS2_OK;
 }

@@ -23,9 +23,9 @@
 //                  kind::f8f6f4 for E4M3; M = 128, N = 2 RW, accumulator F32) into
 //                  one of two 256-column TMEM buffers; warps 2-9 drain the
 //                  accumulator (tcgen05.ld), round to the volume type into a
-//                  shared staging tile, write level 0 with coalesced row segments,
-//                  pool level 1 from the two rows of the tile, and levels 2 and 3
-//                  from two-row rings of the levels above.
+//                  shared staging tile, write level 0 in 16-byte chunks aligned in
+//                  global memory, pool level 1 from the two rows of the tile, and
+//                  levels 2 and 3 from two-row rings of the levels above.
 // The volume is never re-read: the HBM traffic is the pyramid's writes plus the
 // operand reads (L2-resident: one frame's operand rows are 848 KB at 43x77).
 //
@@ -41,6 +41,7 @@ namespace {
 
 constexpr int kCvC = 128;          // feature channels (K of the contraction)
 constexpr int kCvMaxW = 96;        // widest image row a B box holds
+constexpr int kCvMaxRW = 96;       // round_up(kCvMaxW, 16): accumulator columns per image row
 constexpr int kCvThreads = 320;    // 10 warps: TMA, MMA, 8 epilogue
 constexpr int kCvEpiThreads = 256;
 constexpr int kCvStages = 2;
@@ -66,7 +67,7 @@ struct CvGeom {
   int levels, mtiles, ntiles;
   int64_t E;
   uint32_t sub_b;                  // bytes of one B sub-tile (2 RW rows x 128 B)
-  uint32_t off_b, off_stg, off_r1, off_r2, off_r3, off_bar, smem;
+  uint32_t off_b, off_stg, off_r1, off_r2, off_bar, smem;
 };
 
 CvGeom cv_geom(int H, int W, int64_t E, int levels, int esub) {
@@ -75,7 +76,7 @@ CvGeom cv_geom(int H, int W, int64_t E, int levels, int esub) {
   g.W = W;
   g.HW = H * W;
   g.RW = (W + 15) & ~15;
-  g.SST = 2 * g.RW + 8;
+  g.SST = 2 * g.RW + 2;                 // >= 2 W; SST / 2 odd
   g.H1 = H / 2, g.W1 = W / 2, g.H2 = g.H1 / 2, g.W2 = g.W1 / 2, g.H3 = g.H2 / 2, g.W3 = g.W2 / 2;
   g.levels = levels;
   g.mtiles = (g.HW + 127) / 128;
@@ -87,8 +88,7 @@ CvGeom cv_geom(int H, int W, int64_t E, int levels, int esub) {
   g.off_stg = g.off_b + kCvStages * esub * g.sub_b;
   g.off_r1 = g.off_stg + 128u * g.SST * 2;
   g.off_r2 = g.off_r1 + 2u * 128 * (g.RW / 2) * 2;
-  g.off_r3 = g.off_r2 + 2u * 128 * (g.RW / 4) * 2;
-  g.off_bar = (g.off_r3 + 128u * (g.RW / 8) * 2 + 15) & ~15u;
+  g.off_bar = (g.off_r2 + 2u * 128 * (g.RW / 4) * 2 + 15) & ~15u;
   g.smem = g.off_bar + 256 + 1024;   // barriers, flags, TMEM slot; 1 KB alignment slack
   return g;
 }
@@ -102,21 +102,6 @@ template <typename T> __device__ __forceinline__ T from_bits16(uint16_t b);
 template <> __device__ __forceinline__ __half from_bits16<__half>(uint16_t b) { return __ushort_as_half(b); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_bits16<__nv_bfloat16>(uint16_t b) {
   return __ushort_as_bfloat16(b);
-}
-
-// One warp copies n contiguous 16-bit elements from shared memory to global
-// memory, in 4-byte stores where the destination allows (an unaligned first or
-// last element goes alone).
-__device__ __forceinline__ void write_row(uint16_t* dst, const uint16_t* src, int n, int lane) {
-  if (n <= 0) return;
-  const int lead = (int)((reinterpret_cast<uintptr_t>(dst) >> 1) & 1);
-  if (lead && lane == 0) dst[0] = src[0];
-  const int npair = (n - lead) >> 1;
-  for (int k = lane; k < npair; k += 32) {
-    const uint32_t lo = src[lead + 2 * k], hi = src[lead + 2 * k + 1];
-    *reinterpret_cast<uint32_t*>(dst + lead + 2 * k) = lo | (hi << 16);
-  }
-  if (((n - lead) & 1) && lane == 0) dst[n - 1] = src[n - 1];
 }
 
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kCvEpiThreads) : "memory"); }
@@ -224,8 +209,7 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
   uint16_t* stg = reinterpret_cast<uint16_t*>(gb + g.off_stg);
   uint16_t* ring1 = reinterpret_cast<uint16_t*>(gb + g.off_r1);
   uint16_t* ring2 = reinterpret_cast<uint16_t*>(gb + g.off_r2);
-  uint16_t* ring3 = reinterpret_cast<uint16_t*>(gb + g.off_r3);
-  const int R1 = g.RW / 2, R2 = g.RW / 4, R3 = g.RW / 8;   // ring row strides (elements)
+  const int R1 = g.RW / 2, R2 = g.RW / 4;   // ring row strides (elements)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
@@ -337,18 +321,30 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
     }
   } else {
     // ------------------------------------------------------------- epilogue
+    // Phase A (per tile): warp (quarter q, half h) reads its 32 accumulator rows' columns
+    // of image row h from TMEM, rounds them and stores them, 4 bytes at a time, into the
+    // staging row of each source pixel: segment layout, image row 0 at [0, W), row 1 at
+    // [W, 2W) (row stride SST, SST/2 odd: the 32 rows of a store hit 32 banks).
+    // Phase B: warp ew owns staging rows 16 ew .. 16 ew + 15.  Level 0: the row's
+    // segment is one contiguous run of the volume row; it is written in 16-byte chunks
+    // aligned in GLOBAL memory (lane = (row, chunk parity)), each gathered from 8 staged
+    // elements -- whole sectors per store; the two chunks that straddle the segment's
+    // ends go element by element.  Levels 1-3: lanes over x per row, each pooled value
+    // written to its ring and to global memory by the lane that forms it.
     const int ew = warp - 2;                 // 0..7
     const int q = warp & 3;                  // TMEM lane quarter
-    const int h = ew >> 2;                   // which image row of the tile
-    const int et = tid - 64;                 // 0..255
+    const int h = ew >> 2;                   // which image row of the tile (phase A)
     const int r = q * 32 + lane;             // accumulator row = source pixel within the unit
+    const int pa = lane & 15, pb = lane >> 4;
+    const int prow = 16 * ew + pa;           // phase B staging row of this lane
+    const int64_t L1n = (int64_t)g.H1 * g.W1, L2n = (int64_t)g.H2 * g.W2, L3n = (int64_t)g.H3 * g.W3;
     uint32_t gt = 0;
     for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
       const int64_t e = u / g.mtiles;
       const int m0 = (int)(u - e * g.mtiles) * 128;
       const int64_t fi = ii[e], fj = jj[e];
       if (fi < 0 || fi >= K1 || fj < 0 || fj >= K2) {
-        if (et == 0 && m0 == 0) atomicOr(info, HS2_DEV_BAD_INDEX);
+        if (tid == 64 && m0 == 0) atomicOr(info, HS2_DEV_BAD_INDEX);
         continue;
       }
       float sa = 1.f;
@@ -360,25 +356,46 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
         ok = tc::mbar_wait(t_full + 8 * b, (gt >> 1) & 1, abort_flag);
         tc::fence_after();
         if (ok && h < nrow) {
-          for (int c0 = 0; c0 < g.RW; c0 += 16) {
-            uint32_t v[16];
-            tc::ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256 + h * g.RW + c0), v);
-            tc::ld_wait();
-            uint32_t pk[8];
+          uint32_t v[kCvMaxRW];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-              float x0 = __uint_as_float(v[2 * i]), x1 = __uint_as_float(v[2 * i + 1]);
-              if (P == kE4M3) {
-                const int64_t n0 = fj * g.HW + (int64_t)(2 * j + h) * g.W + c0 + 2 * i;
-                const int xw = c0 + 2 * i;
-                x0 = xw < g.W ? (x0 * sa) * s2[n0] : 0.f;
-                x1 = xw + 1 < g.W ? (x1 * sa) * s2[n0 + 1] : 0.f;
-              }
-              pk[i] = (uint32_t)bits16<T>(from_f<T>(x0)) | ((uint32_t)bits16<T>(from_f<T>(x1)) << 16);
+          for (int c0 = 0; c0 < kCvMaxRW; c0 += 16) {
+            if (c0 < g.RW) {
+              uint32_t t16[16];
+              tc::ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256 + h * g.RW + c0), t16);
+#pragma unroll
+              for (int k = 0; k < 16; ++k) v[c0 + k] = t16[k];
             }
-            uint4* dst = reinterpret_cast<uint4*>(stg + r * g.SST + h * g.RW + c0);
-            dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          }
+          tc::ld_wait();
+          if (P == kE4M3) {
+            // column scales of the tile's image row (lane c holds columns c, c+32, c+64)
+            float sc[(kCvMaxRW + 31) / 32];
+#pragma unroll
+            for (int k = 0; k < (kCvMaxRW + 31) / 32; ++k) {
+              const int x = lane + 32 * k;
+              sc[k] = x < g.W ? s2[fj * g.HW + (int64_t)(2 * j + h) * g.W + x] : 0.f;
+            }
+#pragma unroll
+            for (int x = 0; x < kCvMaxRW; ++x) {
+              const float scale = __shfl_sync(0xffffffffu, sc[x >> 5], x & 31);
+              v[x] = __float_as_uint(__uint_as_float(v[x]) * sa * scale);
+            }
+          }
+          uint16_t* srow = stg + r * g.SST + h * g.W;
+          auto q16 = [&](int x) -> uint32_t { return (uint32_t)bits16<T>(from_f<T>(__uint_as_float(v[x]))); };
+          if (((h * g.W) & 1) == 0) {
+#pragma unroll
+            for (int x = 0; x < kCvMaxRW; x += 2) {
+              if (x + 1 < g.W) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
+              else if (x < g.W) srow[x] = (uint16_t)q16(x);
+            }
+          } else {
+            srow[0] = (uint16_t)q16(0);
+#pragma unroll
+            for (int x = 1; x < kCvMaxRW; x += 2) {
+              if (x + 1 < g.W) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
+              else if (x < g.W) srow[x] = (uint16_t)q16(x);
+            }
           }
         }
         tc::fence_before();
@@ -386,56 +403,79 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
         if (lane == 0) tc::mbar_arrive(t_empty + 8 * b);
         ok = epi_sync_and(ok);               // uniform over the epilogue warps from here on
         if (ok) {
-          // level 0: per source row, the tile's nrow image rows are one contiguous run
-          for (int rr = ew; rr < 128; rr += 8) {
-            const int m = m0 + rr;
-            if (m >= g.HW) break;
-            uint16_t* d0 = out.lvl[0] + ((e * g.HW + m) * (int64_t)g.HW + (int64_t)(2 * j) * g.W);
-            write_row(d0, stg + rr * g.SST, g.W, lane);
-            if (nrow == 2) write_row(d0 + g.W, stg + rr * g.SST + g.RW, g.W, lane);
+          // ---- level 0: global-aligned 16-byte chunks of this lane's row
+          const int nseg = nrow * g.W;
+          {
+            const int m = m0 + prow;
+            if (m < g.HW) {
+              const int64_t G0 = (e * g.HW + m) * (int64_t)g.HW + (int64_t)(2 * j) * g.W;
+              const int off = (int)(G0 & 7);
+              const int nch = (off + nseg + 7) >> 3;
+              uint16_t* gb0 = out.lvl[0] + (G0 - off);
+              const uint16_t* sr = stg + prow * g.SST;
+              for (int k = pb; k < nch; k += 2) {
+                const int c0 = 8 * k - off;
+                if (c0 >= 0 && c0 + 8 <= nseg) {
+                  uint32_t wv[4];
+#pragma unroll
+                  for (int i = 0; i < 4; ++i) wv[i] = (uint32_t)sr[c0 + 2 * i] | ((uint32_t)sr[c0 + 2 * i + 1] << 16);
+                  *reinterpret_cast<uint4*>(gb0 + 8 * k) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                } else {
+#pragma unroll
+                  for (int i = 0; i < 8; ++i) {
+                    const int c = c0 + i;
+                    if (c >= 0 && c < nseg) gb0[8 * k + i] = sr[c];
+                  }
+                }
+              }
+            }
           }
+          // ---- levels 1-3: rows 16 ew .. 16 ew + 15, lanes over x
           if (g.levels > 1 && j < g.H1) {
             uint16_t* r1 = ring1 + (j & 1) * 128 * R1;
-            for (int it = et; it < 128 * g.W1; it += kCvEpiThreads) {
-              const int rr = it / g.W1, x = it - rr * g.W1;
-              const uint16_t* s = stg + rr * g.SST + 2 * x;
-              r1[rr * R1 + x] = pool4<T>(s[0], s[1], s[g.RW], s[g.RW + 1]);
+            for (int a2 = 0; a2 < 16; ++a2) {
+              const int rr = 16 * ew + a2;
+              const int m = m0 + rr;
+              const uint16_t* sr = stg + rr * g.SST;
+              for (int x = lane; x < g.W1; x += 32) {
+                const uint16_t pv = pool4<T>(sr[2 * x], sr[2 * x + 1], sr[g.W + 2 * x], sr[g.W + 2 * x + 1]);
+                r1[rr * R1 + x] = pv;
+                if (m < g.HW) out.lvl[1][(e * g.HW + m) * L1n + (int64_t)j * g.W1 + x] = pv;
+              }
             }
-            epi_sync();
-            const int64_t L1 = (int64_t)g.H1 * g.W1;
-            for (int rr = ew; rr < 128 && m0 + rr < g.HW; rr += 8)
-              write_row(out.lvl[1] + ((e * g.HW + m0 + rr) * L1 + (int64_t)j * g.W1), r1 + rr * R1, g.W1, lane);
+            __syncwarp();
             const int j2 = j >> 1;
             if (g.levels > 2 && (j & 1) && j2 < g.H2) {
               uint16_t* r2 = ring2 + (j2 & 1) * 128 * R2;
-              for (int it = et; it < 128 * g.W2; it += kCvEpiThreads) {
-                const int rr = it / g.W2, x = it - rr * g.W2;
-                const uint16_t* a = ring1 + rr * R1 + 2 * x;             // L1 row j-1 (slot 0)
-                const uint16_t* c = ring1 + 128 * R1 + rr * R1 + 2 * x;  // L1 row j (slot 1)
-                r2[rr * R2 + x] = pool4<T>(a[0], a[1], c[0], c[1]);
+              for (int a2 = 0; a2 < 16; ++a2) {
+                const int rr = 16 * ew + a2;
+                const int m = m0 + rr;
+                const uint16_t* p0 = ring1 + rr * R1;              // level-1 row j-1 (slot 0)
+                const uint16_t* p1 = ring1 + 128 * R1 + rr * R1;   // level-1 row j (slot 1)
+                for (int x = lane; x < g.W2; x += 32) {
+                  const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
+                  r2[rr * R2 + x] = pv;
+                  if (m < g.HW) out.lvl[2][(e * g.HW + m) * L2n + (int64_t)j2 * g.W2 + x] = pv;
+                }
               }
-              epi_sync();
-              const int64_t L2 = (int64_t)g.H2 * g.W2;
-              for (int rr = ew; rr < 128 && m0 + rr < g.HW; rr += 8)
-                write_row(out.lvl[2] + ((e * g.HW + m0 + rr) * L2 + (int64_t)j2 * g.W2), r2 + rr * R2, g.W2, lane);
+              __syncwarp();
               const int j3 = j2 >> 1;
               if (g.levels > 3 && (j2 & 1) && j3 < g.H3) {
-                for (int it = et; it < 128 * g.W3; it += kCvEpiThreads) {
-                  const int rr = it / g.W3, x = it - rr * g.W3;
-                  const uint16_t* a = ring2 + rr * R2 + 2 * x;
-                  const uint16_t* c = ring2 + 128 * R2 + rr * R2 + 2 * x;
-                  ring3[rr * R3 + x] = pool4<T>(a[0], a[1], c[0], c[1]);
+                for (int a2 = 0; a2 < 16; ++a2) {
+                  const int rr = 16 * ew + a2;
+                  const int m = m0 + rr;
+                  const uint16_t* p0 = ring2 + rr * R2;
+                  const uint16_t* p1 = ring2 + 128 * R2 + rr * R2;
+                  for (int x = lane; x < g.W3; x += 32) {
+                    const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
+                    if (m < g.HW) out.lvl[3][(e * g.HW + m) * L3n + (int64_t)j3 * g.W3 + x] = pv;
+                  }
                 }
-                epi_sync();
-                const int64_t L3 = (int64_t)g.H3 * g.W3;
-                for (int rr = ew; rr < 128 && m0 + rr < g.HW; rr += 8)
-                  write_row(out.lvl[3] + ((e * g.HW + m0 + rr) * L3 + (int64_t)j3 * g.W3), ring3 + rr * R3, g.W3,
-                            lane);
               }
             }
           }
         }
-        epi_sync();
+        epi_sync();                          // the staging tile is rewritten by the next tile
         if (!ok) break;
       }
       if (!ok) break;

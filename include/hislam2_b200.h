@@ -116,6 +116,12 @@ int hs2_ba_batch_prepare(const hs2_ba_window* windows, int num_windows, int gram
                          void* workspace, size_t workspace_bytes, int* grid, hs2_stream_t stream);
 int hs2_ba_batch_run(void* workspace, int num_windows, int grid, int iterations, float lm, float ep,
                      hs2_stream_t stream);
+/* Test hook of the batched kernel's bounded waits (current device, synchronous):
+ * spin_limit polls before a dependency wait gives up (0 = the default, about a
+ * second); unsatisfiable != 0 makes every wait need one completion more than can
+ * happen, so that each runs out and the launch reports HS2_DEV_TIMEOUT in every
+ * window's info.  Reset with (0, 0). */
+int hs2_ba_batch_set_wait_test(unsigned spin_limit, int unsatisfiable);
 
 /* ---------------------------------------------------------------------------
  * ba_adjoint  (no operator of the reference: HI-SLAM2 differentiates its BA only

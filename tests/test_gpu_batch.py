@@ -129,3 +129,27 @@ def test_batch_reports_a_bad_window(cuda):
     ws[1]["jj"][0] = ws[1]["t1"]            # an edge index >= t1
     with pytest.raises(RuntimeError, match="window 1"):
         backends.BABatch(ws, 1e-4, 0.1)
+
+
+def test_batch_bounded_wait_runs_out_and_reports(cuda):
+    """A dependency wait that nothing can satisfy gives up after its poll limit: the
+    launch drains, every window reports HS2_DEV_TIMEOUT (RuntimeError), and the context
+    stays usable for the next call."""
+    from hislam2_b200 import _lib
+    lib = _lib.load()
+    ws = [on(w, cuda) for w in synth.make_batch_problems(num_windows=4, seed=5)]
+    plan = backends.BABatch(ws, 1e-4, 0.1)
+    try:
+        _lib.check(lib.hs2_ba_batch_set_wait_test(1000, 1), "ba_batch_set_wait_test")
+        plan.run(1)
+        torch.cuda.synchronize()
+    finally:
+        _lib.check(lib.hs2_ba_batch_set_wait_test(0, 0), "ba_batch_set_wait_test")
+    with pytest.raises(RuntimeError, match="timed out"):
+        plan.check()
+    fresh = [on(w, cuda) for w in synth.make_batch_problems(num_windows=4, seed=5)]
+    plan2 = backends.BABatch(fresh, 1e-4, 0.1)
+    plan2.run(1)
+    plan2.check()
+    po, _, _, _ = single(synth.make_batch_problems(num_windows=4, seed=5)[0], cuda, 1)
+    assert rel(fresh[0]["poses"], po) < RTOL

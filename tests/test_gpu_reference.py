@@ -192,7 +192,7 @@ def test_corr_lookup_frontend_window_matches_live_reference(cuda, ref_ops, dtype
         # the reference op indexes with 32-bit accessors: level 0 of 258 edges (2.8e9
         # elements) is fed to it in two halves
         ref = torch.cat([ref_ops.corr_index_forward(vol[a:b], crd[a:b], r)[0] for a, b in halves(vol.shape[0])])
-        assert ours.shape == ref.shape == (vol.shape[0], (2 * r + 1) ** 2) + vol.shape[1:3]
+        assert ours.shape == ref.shape == (vol.shape[0], 2 * r + 1, 2 * r + 1) + vol.shape[1:3]
         errs.append(rel(ours, ref))
         g = torch.randn(ours.shape, device=cuda, generator=torch.Generator(cuda).manual_seed(lvl)).to(dtype)
         vg_ours, = droid_backends.corr_index_backward(vol, crd, g, r)
