@@ -306,7 +306,7 @@ def run_ours(args, world, rank, local):
     cpu, acc = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(p, target_seconds=12.0)
-        acc = accuracy_vs_fp64(p, dev)
+        acc = accuracy_vs_fp64(p, dev, args.steps)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -577,25 +577,45 @@ def cpu_baseline(p, target_seconds):
                       "extrapolated linearly in rows (%.1f s)" % (r1, r2, H, t1, t2, full)}
 
 
-def accuracy_vs_fp64(p, dev, iters=2):
+def accuracy_vs_fp64(p, dev, steps, iters=2):
     """Pose / disparity error of ba on the backend300 window after `iters` GN iterations
-    against the float64 oracle (the checker), max |x - x_fp64| / max |x_fp64|."""
+    against the float64 oracle (the checker), max |x - x_fp64| / max |x_fp64|, for both
+    precisions of the tensor-core Schur Gram: 3xTF32 (the FP32 form, the default) and one
+    TF32 product (the mixed form), each with its own device-timed GN iterations / s."""
     import droid_backends
     import oracle
+    from hislam2_b200 import _lib
     q = {k: (v.to(dev) if torch.is_tensor(v) else v) for k, v in p.items()}
-    poses, disps = q["poses"].clone(), q["disps"].clone()
-    droid_backends.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"], q["jj"],
-                      q["t0"], q["t1"], iters, q["lm"], q["ep"], False)
-    torch.cuda.synchronize()
     f = lambda k: p[k].double().cpu().numpy()  # noqa: E731
     t = time.perf_counter()
     r = oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
                      p["ii"].cpu().numpy(), p["jj"].cpu().numpy(), p["t0"], p["t1"], iters, p["lm"], p["ep"])
     dt = time.perf_counter() - t
     rel = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())  # noqa: E731
-    return {"iterations": iters, "pose_err_vs_fp64": rel(poses.double().cpu().numpy(), r.poses),
-            "disp_err_vs_fp64": rel(disps.double().cpu().numpy(), r.disps),
-            "definition": "max |x - x_fp64| / max |x_fp64| over the [300,7] poses / [300,43,77] disparities",
+    poses, disps = q["poses"].clone(), q["disps"].clone()
+
+    def call(n):
+        poses.copy_(q["poses"])
+        disps.copy_(q["disps"])
+        droid_backends.ba(poses, disps, q["intrinsics"], q["targets"], q["weights"], q["eta"], q["ii"], q["jj"],
+                          q["t0"], q["t1"], n, q["lm"], q["ep"], False)
+
+    forms = {}
+    try:
+        for name, prec in (("fp32_3xtf32_gram", 1), ("mixed_1xtf32_gram", 0)):
+            _lib.set_gram_precision(prec)
+            call(iters)
+            torch.cuda.synchronize()
+            err = {"pose_err_vs_fp64": rel(poses.double().cpu().numpy(), r.poses),
+                   "disp_err_vs_fp64": rel(disps.double().cpu().numpy(), r.disps)}
+            ms = device_time(lambda: call(p["iters"]), steps)
+            forms[name] = dict(err, gn_iters_per_s=round(p["iters"] * 1e3 / ms, 2))
+    finally:
+        _lib.set_gram_precision(1)
+    return {"iterations": iters, "forms": forms,
+            "definition": "max |x - x_fp64| / max |x_fp64| over the [300,7] poses / [300,43,77] disparities "
+                          "after %d GN iterations; gn_iters_per_s device-timed at %d iterations per call"
+                          % (iters, p["iters"]),
             "oracle_seconds": round(dt, 1)}
 
 

@@ -48,6 +48,7 @@ SIGNATURES = {
     "hs2_ba_reduced_system": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32,
                               _i32, _p, _p, _p, _p, _sz, _p],
     "hs2_ba_set_schur_path": [_i32],
+    "hs2_ba_set_gram_precision": [_i32],
     "hs2_ba_adjoint_workspace_size": [_i64, _i64, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_sz)],
     "hs2_ba_adjoint": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _i64, _p, _p, _i64, _i32, _i32, _f32, _f32,
                        _p, _p, _p, _i64, _p, _p, _p, _p, _p, _p, _sz, _p],
@@ -129,6 +130,11 @@ def profile_report(reset=True):
 def launch_count():
     """Kernels launched by the library so far in this process."""
     return int(load().hs2_launch_count())
+
+
+def set_gram_precision(precision):
+    """1: 3xTF32 tensor-core Gram (FP32-accurate, default); 0: one TF32 product (mixed form)."""
+    check(load().hs2_ba_set_gram_precision(int(precision)), "ba_set_gram_precision")
 
 
 def set_schur_path(path):

@@ -756,7 +756,7 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, BaPtrs w, int P,
-                   int32_t* __restrict__ info) {
+                   int32_t* __restrict__ info, int split3) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
@@ -855,9 +855,13 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
           const int r = rb + u * kTcSplitWarps;
           if (r < Npad) {
             const uint32_t o = sw128_off(r, lane);
-            const float gh = tf32_hi(g[u]);
-            *reinterpret_cast<float*>(hi + o) = gh;
-            *reinterpret_cast<float*>(lo + o) = g[u] - gh;
+            if (split3) {
+              const float gh = tf32_hi(g[u]);
+              *reinterpret_cast<float*>(hi + o) = gh;
+              *reinterpret_cast<float*>(lo + o) = g[u] - gh;
+            } else {
+              *reinterpret_cast<float*>(hi + o) = g[u];   // one TF32 product: the MMA reads the top bits
+            }
           }
         }
       }
@@ -886,8 +890,10 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
         for (int k = 0; k < kTcK / 8; ++k) {
           const uint32_t kb = k * 32;
           umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_hi + boff + kb), idesc, (c | k) ? 1u : 0u);
-          umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + boff + kb), idesc, 1u);
-          umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + boff + kb), idesc, 1u);
+          if (split3) {
+            umma_tf32(d, umma_desc_sw128(a_hi + kb), umma_desc_sw128(b_lo + boff + kb), idesc, 1u);
+            umma_tf32(d, umma_desc_sw128(a_lo + kb), umma_desc_sw128(b_hi + boff + kb), idesc, 1u);
+          }
         }
       }
       umma_commit(bar_empty + 8 * st);
@@ -2159,6 +2165,9 @@ struct BaLaunch {
 //      frames of at most kFMaxEdges edges and kFMaxRows Schur rows, the unfused
 //      linearisation + SIMT Gram for the others, back-substitution recomputing E.
 static std::atomic<int> g_schur_path{0};
+// Precision of the tensor-core Gram: 1 = 3xTF32 (hi.hi + hi.lo + lo.hi, FP32-accurate,
+// the default), 0 = one TF32 product (the reduced-precision Hessian of the mixed form).
+static std::atomic<int> g_gram_split3{1};
 
 static BaLaunch ba_launch_shape(const BaProblem& p) {
   BaLaunch l;
@@ -2252,7 +2261,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
       rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
       if (rc) return rc;
       dim3 grid((unsigned)S, 1u, l.tc_split);
-      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info);
+      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info, g_gram_split3.load());
       HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
     }
     dim3 grid((unsigned)S, l.schur_split);
@@ -2397,6 +2406,16 @@ extern "C" int hs2_ba_reduced_system(const float* poses, int64_t num_poses, cons
     HS2_CUDA(cudaMemcpyAsync(A_out, w.A, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
     HS2_CUDA(cudaMemcpyAsync(b_out, w.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   }
+  return HS2_OK;
+}
+
+extern "C" int hs2_ba_set_gram_precision(int precision) {
+  using namespace hs2;
+  if (precision != 0 && precision != 1) {
+    set_error("ba_set_gram_precision: 1 (3xTF32, FP32-accurate) or 0 (one TF32 product)");
+    return HS2_ERR_INVALID;
+  }
+  g_gram_split3.store(precision);
   return HS2_OK;
 }
 

@@ -42,8 +42,10 @@ namespace {
 constexpr int kCvC = 128;          // feature channels (K of the contraction)
 constexpr int kCvMaxW = 96;        // widest image row a B box holds
 constexpr int kCvMaxRW = 96;       // round_up(kCvMaxW, 16): accumulator columns per image row
-constexpr int kCvThreads = 320;    // 10 warps: TMA, MMA, 8 epilogue
-constexpr int kCvEpiThreads = 256;
+constexpr int kCvEpiWarps = 16;    // four per TMEM lane quarter
+constexpr int kCvThreads = 32 * (2 + kCvEpiWarps);   // TMA, MMA, epilogue
+constexpr int kCvEpiThreads = 32 * kCvEpiWarps;
+constexpr int kCvRowsPerWarp = 128 / kCvEpiWarps;   // staging rows of a warp in phase B
 constexpr int kCvStages = 2;
 constexpr int kCvTmemCols = 512;   // two 256-column accumulators
 constexpr uint32_t kCvASub = 128 * 128;   // one 128-row x 128-byte swizzled sub-tile
@@ -221,7 +223,7 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(t_full + 8 * b, 1);
-      tc::mbar_init(t_empty + 8 * b, 8);
+      tc::mbar_init(t_empty + 8 * b, kCvEpiWarps);
     }
     tc::mbar_init(mma_done, 1);
     *abort_flag = 0;
@@ -331,12 +333,15 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
     // elements -- whole sectors per store; the two chunks that straddle the segment's
     // ends go element by element.  Levels 1-3: lanes over x per row, each pooled value
     // written to its ring and to global memory by the lane that forms it.
-    const int ew = warp - 2;                 // 0..7
+    const int ew = warp - 2;                 // 0..15
     const int q = warp & 3;                  // TMEM lane quarter
-    const int h = ew >> 2;                   // which image row of the tile (phase A)
+    const int h = (ew >> 2) >> 1;            // image row of the tile (phase A)
+    const int half = (ew >> 2) & 1;          // which half of the row's RW columns
+    const int hw = g.RW / 2;                 // columns per warp (a multiple of 8)
     const int r = q * 32 + lane;             // accumulator row = source pixel within the unit
-    const int pa = lane & 15, pb = lane >> 4;
-    const int prow = 16 * ew + pa;           // phase B staging row of this lane
+    const int pa = lane % kCvRowsPerWarp, pb = lane / kCvRowsPerWarp;
+    const int prow = kCvRowsPerWarp * ew + pa;   // phase B staging row of this lane
+    constexpr int kChunkLanes = 32 / kCvRowsPerWarp;
     const int64_t L1n = (int64_t)g.H1 * g.W1, L2n = (int64_t)g.H2 * g.W2, L3n = (int64_t)g.H3 * g.W3;
     uint32_t gt = 0;
     for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
@@ -356,45 +361,48 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
         ok = tc::mbar_wait(t_full + 8 * b, (gt >> 1) & 1, abort_flag);
         tc::fence_after();
         if (ok && h < nrow) {
-          uint32_t v[kCvMaxRW];
+          constexpr int kHalf = kCvMaxRW / 2;
+          uint32_t v[kHalf];
 #pragma unroll
-          for (int c0 = 0; c0 < kCvMaxRW; c0 += 16) {
-            if (c0 < g.RW) {
-              uint32_t t16[16];
-              tc::ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256 + h * g.RW + c0), t16);
+          for (int c0 = 0; c0 < kHalf; c0 += 8) {
+            if (c0 < hw) {
+              uint32_t t8[8];
+              tc::ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256 + h * g.RW + half * hw + c0), t8);
 #pragma unroll
-              for (int k = 0; k < 16; ++k) v[c0 + k] = t16[k];
+              for (int k = 0; k < 8; ++k) v[c0 + k] = t8[k];
             }
           }
           tc::ld_wait();
+          const int xb = half * hw;          // first image column of this warp
           if (P == kE4M3) {
-            // column scales of the tile's image row (lane c holds columns c, c+32, c+64)
-            float sc[(kCvMaxRW + 31) / 32];
+            // column scales of the warp's columns (lane c holds columns xb + c, xb + c + 32)
+            float sc[(kHalf + 31) / 32];
 #pragma unroll
-            for (int k = 0; k < (kCvMaxRW + 31) / 32; ++k) {
-              const int x = lane + 32 * k;
-              sc[k] = x < g.W ? s2[fj * g.HW + (int64_t)(2 * j + h) * g.W + x] : 0.f;
+            for (int k = 0; k < (kHalf + 31) / 32; ++k) {
+              const int x = xb + lane + 32 * k;
+              sc[k] = (lane + 32 * k < hw && x < g.W) ? s2[fj * g.HW + (int64_t)(2 * j + h) * g.W + x] : 0.f;
             }
 #pragma unroll
-            for (int x = 0; x < kCvMaxRW; ++x) {
+            for (int x = 0; x < kHalf; ++x) {
               const float scale = __shfl_sync(0xffffffffu, sc[x >> 5], x & 31);
               v[x] = __float_as_uint(__uint_as_float(v[x]) * sa * scale);
             }
           }
-          uint16_t* srow = stg + r * g.SST + h * g.W;
+          uint16_t* srow = stg + r * g.SST + h * g.W + xb;
+          const int nv = min(hw, g.W - xb);   // valid columns of this warp
           auto q16 = [&](int x) -> uint32_t { return (uint32_t)bits16<T>(from_f<T>(__uint_as_float(v[x]))); };
-          if (((h * g.W) & 1) == 0) {
+          if (((h * g.W + xb) & 1) == 0) {
 #pragma unroll
-            for (int x = 0; x < kCvMaxRW; x += 2) {
-              if (x + 1 < g.W) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
-              else if (x < g.W) srow[x] = (uint16_t)q16(x);
+            for (int x = 0; x < kHalf; x += 2) {
+              if (x + 1 < nv) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
+              else if (x < nv) srow[x] = (uint16_t)q16(x);
             }
           } else {
-            srow[0] = (uint16_t)q16(0);
+            if (nv > 0) srow[0] = (uint16_t)q16(0);
 #pragma unroll
-            for (int x = 1; x < kCvMaxRW; x += 2) {
-              if (x + 1 < g.W) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
-              else if (x < g.W) srow[x] = (uint16_t)q16(x);
+            for (int x = 1; x < kHalf; x += 2) {
+              if (x + 1 < nv) *reinterpret_cast<uint32_t*>(srow + x) = q16(x) | (q16(x + 1) << 16);
+              else if (x < nv) srow[x] = (uint16_t)q16(x);
             }
           }
         }
@@ -413,7 +421,7 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
               const int nch = (off + nseg + 7) >> 3;
               uint16_t* gb0 = out.lvl[0] + (G0 - off);
               const uint16_t* sr = stg + prow * g.SST;
-              for (int k = pb; k < nch; k += 2) {
+              for (int k = pb; k < nch; k += kChunkLanes) {
                 const int c0 = 8 * k - off;
                 if (c0 >= 0 && c0 + 8 <= nseg) {
                   uint32_t wv[4];
@@ -433,43 +441,50 @@ corr_volume_kernel(const __grid_constant__ CUtensorMap amap, const __grid_consta
           // ---- levels 1-3: rows 16 ew .. 16 ew + 15, lanes over x
           if (g.levels > 1 && j < g.H1) {
             uint16_t* r1 = ring1 + (j & 1) * 128 * R1;
-            for (int a2 = 0; a2 < 16; ++a2) {
-              const int rr = 16 * ew + a2;
-              const int m = m0 + rr;
+            const int rbase = kCvRowsPerWarp * ew;
+            // items (row, x) of the warp's rows, lane-strided, stepped without division
+            int a2 = 0, x = lane;
+            while (x >= g.W1) { x -= g.W1; ++a2; }
+            for (; a2 < kCvRowsPerWarp;) {
+              const int rr = rbase + a2;
               const uint16_t* sr = stg + rr * g.SST;
-              for (int x = lane; x < g.W1; x += 32) {
-                const uint16_t pv = pool4<T>(sr[2 * x], sr[2 * x + 1], sr[g.W + 2 * x], sr[g.W + 2 * x + 1]);
-                r1[rr * R1 + x] = pv;
-                if (m < g.HW) out.lvl[1][(e * g.HW + m) * L1n + (int64_t)j * g.W1 + x] = pv;
-              }
+              const uint16_t pv = pool4<T>(sr[2 * x], sr[2 * x + 1], sr[g.W + 2 * x], sr[g.W + 2 * x + 1]);
+              r1[rr * R1 + x] = pv;
+              if (m0 + rr < g.HW) out.lvl[1][(e * g.HW + m0 + rr) * L1n + (int64_t)j * g.W1 + x] = pv;
+              x += 32;
+              while (x >= g.W1) { x -= g.W1; ++a2; }
             }
             __syncwarp();
             const int j2 = j >> 1;
             if (g.levels > 2 && (j & 1) && j2 < g.H2) {
               uint16_t* r2 = ring2 + (j2 & 1) * 128 * R2;
-              for (int a2 = 0; a2 < 16; ++a2) {
-                const int rr = 16 * ew + a2;
-                const int m = m0 + rr;
+              a2 = 0;
+              x = lane;
+              while (x >= g.W2) { x -= g.W2; ++a2; }
+              for (; a2 < kCvRowsPerWarp;) {
+                const int rr = rbase + a2;
                 const uint16_t* p0 = ring1 + rr * R1;              // level-1 row j-1 (slot 0)
                 const uint16_t* p1 = ring1 + 128 * R1 + rr * R1;   // level-1 row j (slot 1)
-                for (int x = lane; x < g.W2; x += 32) {
-                  const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
-                  r2[rr * R2 + x] = pv;
-                  if (m < g.HW) out.lvl[2][(e * g.HW + m) * L2n + (int64_t)j2 * g.W2 + x] = pv;
-                }
+                const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
+                r2[rr * R2 + x] = pv;
+                if (m0 + rr < g.HW) out.lvl[2][(e * g.HW + m0 + rr) * L2n + (int64_t)j2 * g.W2 + x] = pv;
+                x += 32;
+                while (x >= g.W2) { x -= g.W2; ++a2; }
               }
               __syncwarp();
               const int j3 = j2 >> 1;
               if (g.levels > 3 && (j2 & 1) && j3 < g.H3) {
-                for (int a2 = 0; a2 < 16; ++a2) {
-                  const int rr = 16 * ew + a2;
-                  const int m = m0 + rr;
+                a2 = 0;
+                x = lane;
+                while (x >= g.W3) { x -= g.W3; ++a2; }
+                for (; a2 < kCvRowsPerWarp;) {
+                  const int rr = rbase + a2;
                   const uint16_t* p0 = ring2 + rr * R2;
                   const uint16_t* p1 = ring2 + 128 * R2 + rr * R2;
-                  for (int x = lane; x < g.W3; x += 32) {
-                    const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
-                    if (m < g.HW) out.lvl[3][(e * g.HW + m) * L3n + (int64_t)j3 * g.W3 + x] = pv;
-                  }
+                  const uint16_t pv = pool4<T>(p0[2 * x], p0[2 * x + 1], p1[2 * x], p1[2 * x + 1]);
+                  if (m0 + rr < g.HW) out.lvl[3][(e * g.HW + m0 + rr) * L3n + (int64_t)j3 * g.W3 + x] = pv;
+                  x += 32;
+                  while (x >= g.W3) { x -= g.W3; ++a2; }
                 }
               }
             }

@@ -379,6 +379,16 @@ int hs2_bi_inter(const float* scales, int64_t num, int hs, int ws, const float* 
  */
 int hs2_ba_set_schur_path(int path);
 
+/* Precision of ba's tensor-core Schur Gram (process-wide, default 1; no counterpart
+ * in the reference, whose Gram is FP32 SIMT):
+ *   1 3xTF32 (hi.hi + hi.lo + lo.hi): FP32-accurate Hessian blocks;
+ *   0 one TF32 product per term: the reduced camera system carries about 1e-3 relative
+ *     error while the gradient stays FP32, so Gauss-Newton converges to the same
+ *     point (the mixed-precision form; bench.py reports its pose error).
+ * Applies to the default Schur path (0 of hs2_ba_set_schur_path); frames on the SIMT
+ * Gram (more than 42 Schur rows) and the fused per-frame path keep FP32 accuracy. */
+int hs2_ba_set_gram_precision(int precision);
+
 /* ---------------------------------------------------------------------------
  * Measurement support (no counterpart in the reference, which has no profiler).
  * hs2_profile_enable(1) brackets every kernel launch of this library with CUDA

@@ -209,3 +209,10 @@ def test_corr_reproject_lookup_host_validation():
     empty = list(args)
     empty[14] = 0
     assert lib.hs2_corr_reproject_lookup(*empty) == _lib.HS2_OK
+
+
+def test_gram_precision_setter_validation():
+    lib = _lib.load()
+    assert lib.hs2_ba_set_gram_precision(2) == _lib.HS2_ERR_INVALID
+    assert b"3xTF32" in lib.hs2_last_error()
+    assert lib.hs2_ba_set_gram_precision(1) == _lib.HS2_OK

@@ -50,11 +50,16 @@ def ours(backend300, cuda):
     return poses, disps, dx, dz
 
 
-def test_backend300_matches_fp64_oracle(backend300, ours):
+@pytest.fixture(scope="module")
+def fp64(backend300):
     p = backend300
     f = lambda k: p[k].double().numpy()  # noqa: E731
-    r = oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
-                     p["ii"].numpy(), p["jj"].numpy(), p["t0"], p["t1"], ITERS, p["lm"], p["ep"], trace=True)
+    return oracle.ba.ba(f("poses"), f("disps"), f("intrinsics"), f("targets"), f("weights"), f("eta"),
+                        p["ii"].numpy(), p["jj"].numpy(), p["t0"], p["t1"], ITERS, p["lm"], p["ep"], trace=True)
+
+
+def test_backend300_matches_fp64_oracle(backend300, ours, fp64):
+    r = fp64
     poses, disps, dx, dz = ours
     rdx, rdz = r.traces[0]["dx"], r.traces[0]["dz"]
     pose_err = rel(poses, r.poses)
@@ -85,3 +90,20 @@ def test_backend300_matches_live_reference(backend300, ours, ref_ops, cuda):
     assert rel(do, disps) < 1e-4
     assert rel(xo, dx) < 1e-4
     assert rel(zo.reshape(dz.shape), dz) < 1e-4
+
+
+def test_backend300_mixed_gram_against_fp64(backend300, fp64, cuda):
+    """The mixed form (one TF32 product in the tensor-core Schur Gram, FP32 gradient):
+    the reduced camera system carries about 1e-3 relative error, so each Gauss-Newton step
+    is slightly off; after ITERS iterations the poses must still agree with the FP64
+    oracle within 1e-4 relative to max |pose| (ten times the FP32 form's bar)."""
+    from hislam2_b200 import _lib
+    try:
+        _lib.set_gram_precision(0)
+        poses, disps, _, _ = run(backend300, cuda, ITERS)
+    finally:
+        _lib.set_gram_precision(1)
+    e_pose, e_disp = rel(poses, fp64.poses), rel(disps, fp64.disps)
+    print("backend300 mixed Gram, %d GN iterations: pose err %.2e, disp err %.2e vs FP64" % (ITERS, e_pose, e_disp))
+    assert e_pose < 1e-4
+    assert e_disp < 1e-3
