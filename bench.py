@@ -296,6 +296,7 @@ def run_ours(args, world, rank, local):
 
     corr = corr_lookup(args, dev, world, peaks)
     pg = pgba_leg(args, dev, world, rank)
+    alt = altcorr_leg(args, dev, world, peaks)
     vol = volume_leg(args, dev, world, peaks) if world == 1 else None
     bat = batch_leg(args, dev, world, rank)
 
@@ -316,7 +317,7 @@ def run_ours(args, world, rank, local):
                 "config": dict(CONFIG, parallelism="replicas: one independent window per rank" if world > 1 else
                                "single GPU"),
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "accuracy": acc, "corr_lookup": corr, "corr_volume": vol, "batch": bat, "pgba": pg, "clocks": clk,
+                "accuracy": acc, "corr_lookup": corr, "altcorr": alt, "corr_volume": vol, "batch": bat, "pgba": pg, "clocks": clk,
                 "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
                 "library_peaks_tflops": {"sgemm_fp32": round(simt[0], 2), "dgemm_fp64": round(simt[1], 2)}}
         print(json.dumps(line), flush=True)
@@ -489,6 +490,50 @@ def batch_leg(args, dev, world, rank):
             "sequential_single_window_ms_per_iteration": round(ms_seq / iters, 4),
             "speedup_vs_sequential": round(ms_seq / ms, 2),
             "config": "64 windows, keyframes U{8..40}, edges U{20..500}, 43x77 or 30x40 grids, t0=1, lm=1e-4, ep=0.1"}
+
+
+def altcorr_leg(args, dev, world, peaks):
+    """The backend's memory-light correlation (AltCorrBlock, radius 3, 4 levels) over all
+    6000 edges of the 300-keyframe window, called in the global BA loop's chunks: the edges
+    whose source frame lies in [i, i + 2) (HI-SLAM2 factor_graph.py:253-260).  One step =
+    one pass over every chunk and level (fp16 features, float32 coordinates)."""
+    from hislam2_b200 import backends, synth
+    from hislam2_b200.corr import _pool_pyramid
+    p = synth.make_ba_problem(WORKLOAD, seed=0)
+    g = torch.Generator().manual_seed(17)
+    K, H, W, C, r, L = 300, 43, 77, 128, 3, 4
+    fmaps = (torch.randn(K, C, H, W, generator=g) / np.sqrt(C)).half().to(dev)
+    pyr = [lv[None].contiguous() for lv in _pool_pyramid(fmaps, L)]
+    ii, jj = p["ii"].to(dev), p["jj"].to(dev)
+    coords = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], p["ii"], p["jj"]).float()
+    coords = (coords + torch.randn(coords.shape, generator=g)).permute(0, 3, 1, 2).contiguous().to(dev)
+    chunks = []
+    for i in range(0, int(p["jj"].max()) + 1, 2):
+        v = ((ii >= i) & (ii < i + 2)).nonzero().flatten()
+        if v.numel():
+            chunks.append((ii[v].contiguous(), jj[v].contiguous(),
+                           [(coords[v] / 2 ** lvl)[None].contiguous() for lvl in range(L)]))
+
+    def step():
+        for ci, cj, crd in chunks:
+            for lvl in range(L):
+                backends.altcorr_forward(pyr[0], pyr[lvl], crd[lvl], ci, cj, r)
+
+    steps = max(3, min(args.steps, 10))
+    barrier(world)
+    ms = max_over_ranks(device_time(step, steps), world, dev)
+    E = ii.numel()
+    taps = (2 * r + 1) ** 2
+    flops = sum(2.0 * E * H * W * taps * C for _ in range(L))
+    out_bytes = E * H * W * taps * L * 2
+    res = {"config": "300 keyframes, 6000 edges, 43x77, 128 channels fp16, radius 3, 4 levels, %d chunks of "
+                     "two source frames" % len(chunks),
+           "ms_per_pass": round(ms, 3), "edges_per_s": round(E / (ms / 1e3) * world, 1),
+           "tflops_fp32_simt": round(flops / (ms / 1e3) / 1e12, 2), "write_gbs": round(out_bytes / (ms / 1e3) / 1e9, 1),
+           "algorithmic": {"gflop": round(flops / 1e9, 1), "write_gb": round(out_bytes / 1e9, 3)}}
+    del pyr, chunks
+    torch.cuda.empty_cache()
+    return res
 
 
 def pgba_leg(args, dev, world, rank):

@@ -36,6 +36,10 @@ SIGNATURES = {
                         _p],
     "hs2_altcorr_forward": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _p,
                             _i32, _i32, _p, _p, _p],
+    "hs2_altcorr_pack_workspace_size": [_i32, _i32, _i32, _i32, _i32, _i32, ctypes.POINTER(_sz)],
+    "hs2_altcorr_pack": [_p, _i32, _i32, _i32, _i32, _i32, _i32, _p, _i32, _p, _sz, _p],
+    "hs2_altcorr_forward_packed": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _p,
+                                   _i32, _i32, _p, _p, _p],
     "hs2_altcorr_backward_workspace_size": [_i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32,
                                             ctypes.POINTER(_sz)],
     "hs2_altcorr_backward": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _p, _p, _p,

@@ -708,11 +708,66 @@ def _altcorr_check(fmap1, fmap2, coords, ii, jj):
     return _corr_dtype("fmap1", fmap1)
 
 
-def altcorr_forward(fmap1, fmap2, coords, ii, jj, radius):
+PACKED_CHANNELS = (32, 64, 128, 256)
+
+
+class PackedFeatures:
+    """Channel-last copy ([B, N, H*W, C]) of a [B, N, C, H, W] float16 / bfloat16 feature
+    tensor for :func:`altcorr_forward_packed`; only the listed frames are written."""
+
+    def __init__(self, fmap, frames=None):
+        _contig("fmap", fmap)
+        dt = _corr_dtype("fmap", fmap)
+        if dt not in (_lib.HS2_F16, _lib.HS2_BF16) or fmap.dim() != 5:
+            raise RuntimeError("altcorr_pack: [B,N,C,H,W] float16 or bfloat16 features expected")
+        B, N, C, H, W = fmap.shape
+        n = ctypes.c_size_t(0)
+        lib = _lib.load()
+        _lib.check(lib.hs2_altcorr_pack_workspace_size(dt, B, N, C, H, W, ctypes.byref(n)), "altcorr_pack")
+        self.buf = torch.empty(n.value, dtype=torch.uint8, device=fmap.device)
+        if frames is not None:
+            frames = frames.contiguous()
+            _cuda("frames", frames, fmap.device)
+            _dtype("frames", frames, torch.int64)
+        _lib.check(lib.hs2_altcorr_pack(_ptr(fmap), dt, B, N, C, H, W, _ptr(frames) if frames is not None else None,
+                                        0 if frames is None else frames.numel(), _ptr(self.buf), n.value,
+                                        _stream(fmap.device)), "altcorr_pack")
+        self.dtype, self.torch_dtype, self.shape, self.device = dt, fmap.dtype, tuple(fmap.shape), fmap.device
+
+
+def altcorr_forward_packed(packed1, packed2, coords, ii, jj, radius):
+    """:func:`altcorr_forward` on :class:`PackedFeatures` (float16 / bfloat16, C in 32..256)."""
+    _contig("coords", coords)
+    ii, jj = ii.contiguous(), jj.contiguous()
+    dev = packed1.device
+    for name, t in (("coords", coords), ("ii", ii), ("jj", jj)):
+        _cuda(name, t, dev)
+    _dtype("coords", coords, torch.float32)
+    B, N1, C, H, W = packed1.shape
+    _, N2, C2, H2, W2 = packed2.shape
+    if packed2.dtype != packed1.dtype or C2 != C or packed2.shape[0] != B or coords.dim() != 5 \
+            or tuple(coords.shape[:1]) != (B,) or tuple(coords.shape[2:]) != (2, H, W):
+        raise RuntimeError("altcorr_forward_packed: inconsistent shapes %s %s %s" % (
+            packed1.shape, packed2.shape, tuple(coords.shape)))
+    M = coords.shape[1]
+    if ii.numel() != M or jj.numel() != M:
+        raise RuntimeError("altcorr_forward_packed: ii/jj must have %d entries" % M)
+    r = int(radius)
+    corr = torch.empty(B, M, 2 * r + 1, 2 * r + 1, H, W, dtype=packed1.torch_dtype, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.load().hs2_altcorr_forward_packed(_ptr(packed1.buf), _ptr(packed2.buf), packed1.dtype, B, N1, N2,
+                                                      C, H, W, H2, W2, _ptr(coords), _ptr(ii), _ptr(jj), M, r,
+                                                      _ptr(corr), _ptr(info), _stream(dev)), "altcorr_forward_packed")
+    return [corr]
+
+
+def altcorr_forward(fmap1, fmap2, coords, ii, jj, radius, *, path="auto"):
     """``droid_backends.altcorr_forward`` (reference ``src/droid.cpp:277-289``) -> [corr].
 
     corr is [B, M, 2r+1, 2r+1, H, W] with dim 2 along x, returned contiguous
-    (the reference returns the same values as a permuted view).
+    (the reference returns the same values as a permuted view).  float16 / bfloat16
+    features with C in 32..256 take the channel-last path (the frames of ii / jj packed
+    first) unless ``path="direct"``.
     """
     dt = _altcorr_check(fmap1, fmap2, coords, ii.contiguous(), jj.contiguous())
     ii, jj = ii.contiguous(), jj.contiguous()
@@ -720,6 +775,14 @@ def altcorr_forward(fmap1, fmap2, coords, ii, jj, radius):
     N2, H2, W2 = fmap2.shape[1], fmap2.shape[3], fmap2.shape[4]
     M = coords.shape[1]
     r = int(radius)
+    if path not in ("auto", "direct", "packed"):
+        raise RuntimeError("altcorr_forward: path is auto, direct or packed")
+    packable = dt in (_lib.HS2_F16, _lib.HS2_BF16) and C in PACKED_CHANNELS
+    if path == "packed" and not packable:
+        raise RuntimeError("altcorr_forward: the packed path takes float16 / bfloat16 features with C in %s"
+                           % (PACKED_CHANNELS,))
+    if packable and path != "direct":
+        return altcorr_forward_packed(PackedFeatures(fmap1, ii), PackedFeatures(fmap2, jj), coords, ii, jj, r)
     corr = torch.empty(B, M, 2 * r + 1, 2 * r + 1, H, W, dtype=fmap1.dtype, device=fmap1.device)
     info = torch.zeros(1, dtype=torch.int32, device=fmap1.device)
     _lib.check(_lib.load().hs2_altcorr_forward(_ptr(fmap1), _ptr(fmap2), dt, B, N1, N2, C, H, W, H2, W2,

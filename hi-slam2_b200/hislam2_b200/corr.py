@@ -104,7 +104,13 @@ def _pool_pyramid(fmaps, num_levels):
 
 
 class AltCorrBlock:
-    """Memory-light correlation of HI-SLAM2's backend (reference ``modules/corr.py:90-117``)."""
+    """Memory-light correlation of HI-SLAM2's backend (reference ``modules/corr.py:90-117``).
+
+    For float16 / bfloat16 features with C in 32..256 each pyramid level is also packed
+    channel-last once here, so the per-chunk calls of the backend loop
+    (``factor_graph.py:253-260``) read packed features without re-packing; calls that
+    need gradients go through :class:`CorrLayer`.
+    """
 
     def __init__(self, fmaps, num_levels=4, radius=3):
         self.num_levels = num_levels
@@ -112,13 +118,20 @@ class AltCorrBlock:
         B, N, C, H, W = fmaps.shape
         levels = _pool_pyramid(fmaps.reshape(B * N, C, H, W), num_levels)
         self.pyramid = [lv.view(B, N, C, H // 2 ** i, W // 2 ** i) for i, lv in enumerate(levels)]
+        self.packed = None
+        if fmaps.dtype in (torch.float16, torch.bfloat16) and C in backends.PACKED_CHANNELS and fmaps.is_cuda:
+            self.packed = [backends.PackedFeatures(lv.contiguous()) for lv in self.pyramid]
 
     def __call__(self, coords, ii, jj):
         coords = coords.permute(0, 1, 4, 2, 3).contiguous()
+        grad = torch.is_grad_enabled() and (coords.requires_grad or self.pyramid[0].requires_grad)
         corr_list = []
         for i in range(self.num_levels):
-            corr = CorrLayer.apply(self.pyramid[0], self.pyramid[i].contiguous(), (coords / 2 ** i).contiguous(), ii,
-                                   jj, self.radius)
+            crd = (coords / 2 ** i).contiguous()
+            if self.packed is not None and not grad:
+                corr, = backends.altcorr_forward_packed(self.packed[0], self.packed[i], crd, ii, jj, self.radius)
+            else:
+                corr = CorrLayer.apply(self.pyramid[0], self.pyramid[i].contiguous(), crd, ii, jj, self.radius)
             corr_list.append(corr.flatten(2, 3))
         return torch.stack(corr_list, dim=2).flatten(2, 3)
 

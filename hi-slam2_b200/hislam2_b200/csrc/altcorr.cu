@@ -188,6 +188,154 @@ altcorr_bwd_kernel(const T* __restrict__ fmap1, const T* __restrict__ fmap2, con
   }
 }
 
+// ---------------------------------------------------------------- packed forward ---
+// Fast forward for 16-bit features.  Frames are first packed channel-last ([B, N, HW, C],
+// one 2*C-byte row per pixel), so a window row of D positions is D contiguous rows: a
+// warp computes one pixel's window row by row with lane (position q = lane % 8, channel
+// group g = lane / 8) reading 16-byte chunks of its group's C/4 channels (the eight
+// positions of a chunk step are 8 consecutive rows: coalesced), multiplying in FP32
+// with f16/bf16 operands (fma.rn.f32.f16 / .bf16: exact products, FP32 sums) against
+// the pixel's fmap1 row held in registers, and reducing the four groups by two
+// shuffles.  The window lands in shared memory and the bilinear blend writes the
+// outputs with consecutive threads on consecutive pixels, as in the direct kernel.
+
+// channel-first [B, N, C, H, W] -> channel-last [B, N, HW, C] for the frames whose flag
+// is set (every frame when flags is null); 32 pixels x C channels per CTA through
+// shared memory
+template <typename T>
+__global__ void __launch_bounds__(kAcThreads)
+altcorr_pack_kernel(const T* __restrict__ src, T* __restrict__ dst, const unsigned char* __restrict__ flags, int N,
+                    int C, int HW) {
+  __shared__ T tile[32][257];
+  const int b = blockIdx.z, n = blockIdx.y;
+  if (flags && !flags[n]) return;
+  const int p0 = blockIdx.x * 32;
+  const int np = min(32, HW - p0);
+  const T* s = src + ((int64_t)b * N + n) * C * HW + p0;
+  T* d = dst + (((int64_t)b * N + n) * HW + p0) * C;
+  for (int idx = threadIdx.x; idx < C * 32; idx += kAcThreads) {
+    const int c = idx >> 5, q = idx & 31;
+    if (q < np) tile[q][c] = s[(int64_t)c * HW + q];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < np * C; idx += kAcThreads) {
+    const int q = idx / C, c = idx - q * C;
+    d[(int64_t)q * C + c] = tile[q][c];
+  }
+}
+
+__global__ void altcorr_flag_kernel(const int64_t* __restrict__ idx, int m, int n, unsigned char* __restrict__ flags) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+    const int64_t f = idx[e];
+    if (f >= 0 && f < n) flags[f] = 1;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void dot8(const uint4 a, const uint4 b, float& s0, float& s1);
+
+template <>
+__device__ __forceinline__ void dot8<__half>(const uint4 a, const uint4 b, float& s0, float& s1) {
+  asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t"
+      "mov.b32 {al, ah}, %2;\n\tmov.b32 {bl, bh}, %6;\n\t"
+      "fma.rn.f32.f16 %0, al, bl, %0;\n\tfma.rn.f32.f16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %3;\n\tmov.b32 {bl, bh}, %7;\n\t"
+      "fma.rn.f32.f16 %0, al, bl, %0;\n\tfma.rn.f32.f16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %4;\n\tmov.b32 {bl, bh}, %8;\n\t"
+      "fma.rn.f32.f16 %0, al, bl, %0;\n\tfma.rn.f32.f16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %5;\n\tmov.b32 {bl, bh}, %9;\n\t"
+      "fma.rn.f32.f16 %0, al, bl, %0;\n\tfma.rn.f32.f16 %1, ah, bh, %1;\n\t}"
+      : "+f"(s0), "+f"(s1)
+      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w));
+}
+
+template <>
+__device__ __forceinline__ void dot8<__nv_bfloat16>(const uint4 a, const uint4 b, float& s0, float& s1) {
+  asm("{\n\t.reg .b16 al, ah, bl, bh;\n\t"
+      "mov.b32 {al, ah}, %2;\n\tmov.b32 {bl, bh}, %6;\n\t"
+      "fma.rn.f32.bf16 %0, al, bl, %0;\n\tfma.rn.f32.bf16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %3;\n\tmov.b32 {bl, bh}, %7;\n\t"
+      "fma.rn.f32.bf16 %0, al, bl, %0;\n\tfma.rn.f32.bf16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %4;\n\tmov.b32 {bl, bh}, %8;\n\t"
+      "fma.rn.f32.bf16 %0, al, bl, %0;\n\tfma.rn.f32.bf16 %1, ah, bh, %1;\n\t"
+      "mov.b32 {al, ah}, %5;\n\tmov.b32 {bl, bh}, %9;\n\t"
+      "fma.rn.f32.bf16 %0, al, bl, %0;\n\tfma.rn.f32.bf16 %1, ah, bh, %1;\n\t}"
+      : "+f"(s0), "+f"(s1)
+      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w));
+}
+
+// NCH = C / 32: 16-byte chunks of a lane's channel group per position
+template <typename T, int NCH>
+__global__ void __launch_bounds__(kAcThreads)
+altcorr_fwd_packed_kernel(const T* __restrict__ p1, const T* __restrict__ p2, const float* __restrict__ coords,
+                          const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, T* __restrict__ corr,
+                          int N1, int N2, int H, int W, int H2, int W2, int M, int r, int stride,
+                          int32_t* __restrict__ info) {
+  constexpr int C = 32 * NCH;
+  extern __shared__ float4 smem4[];
+  float4* geo = smem4;                                                   // [kAcPix]
+  float* win = reinterpret_cast<float*>(smem4) + 4 * kAcPix;            // [kAcPix][stride]
+  const int b = blockIdx.z, m = blockIdx.y;
+  const int HW = H * W;
+  const int pix0 = blockIdx.x * kAcPix;
+  const int npix = min(kAcPix, HW - pix0);
+  const int D = 2 * r + 2, rd = 2 * r + 1;
+  const int64_t ix = ii[m], jx = jj[m];
+  const bool ok = ix >= 0 && ix < N1 && jx >= 0 && jx < N2;
+  if (!ok && threadIdx.x == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
+  const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
+  const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
+  for (int q = threadIdx.x; q < npix; q += kAcThreads) {
+    const float x = cx[pix0 + q], y = cy[pix0 + q];
+    const float fx = floorf(x), fy = floorf(y);
+    geo[q] = make_float4(x - fx, y - fy, __int_as_float((int)fx - r), __int_as_float((int)fy - r));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pq = lane & 7, g = lane >> 3;
+  const T* f1 = p1 + ((int64_t)b * N1 + (ok ? ix : 0)) * HW * C;
+  const T* f2 = p2 + ((int64_t)b * N2 + (ok ? jx : 0)) * (int64_t)H2 * W2 * C;
+  for (int q = warp; q < npix; q += kAcThreads / 32) {
+    const float4 gq = geo[q];
+    const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
+    const uint4* a = reinterpret_cast<const uint4*>(f1 + (int64_t)(pix0 + q) * C) + g * NCH;
+    uint4 av[NCH];
+#pragma unroll
+    for (int k = 0; k < NCH; ++k) av[k] = __ldg(a + k);
+    float* wq = win + q * stride;
+    for (int py = 0; py < D; ++py) {
+      const int y1 = yb + py;
+      for (int pc = 0; pc < D; pc += 8) {
+        const int px = pc + pq, x1 = xb + px;
+        float s0 = 0.f, s1 = 0.f;
+        if (ok && px < D && y1 >= 0 && y1 < H2 && x1 >= 0 && x1 < W2) {
+          const uint4* bp = reinterpret_cast<const uint4*>(f2 + ((int64_t)y1 * W2 + x1) * C) + g * NCH;
+#pragma unroll
+          for (int k = 0; k < NCH; ++k) dot8<T>(av[k], __ldg(bp + k), s0, s1);
+        }
+        float sv = s0 + s1;
+        sv += __shfl_xor_sync(0xffffffffu, sv, 8);
+        sv += __shfl_xor_sync(0xffffffffu, sv, 16);
+        if (g == 0 && px < D) wq[py * D + px] = sv * 0.0625f;
+      }
+    }
+  }
+  __syncthreads();
+  const int nout = rd * rd;
+  T* out = corr + ((int64_t)b * M + m) * nout * HW;
+  for (int idx = threadIdx.x; idx < npix * nout; idx += kAcThreads) {
+    const int o = idx / npix;
+    const int q = idx - o * npix;
+    const int a = o / rd;      // x offset (dim 2 of the output)
+    const int bb = o - a * rd; // y offset (dim 3 of the output)
+    const float4 gq = geo[q];
+    const float* w = win + q * stride;
+    const float v = (1.f - gq.x) * (1.f - gq.y) * w[bb * D + a] + gq.x * (1.f - gq.y) * w[bb * D + a + 1] +
+                    (1.f - gq.x) * gq.y * w[(bb + 1) * D + a] + gq.x * gq.y * w[(bb + 1) * D + a + 1];
+    out[(int64_t)o * HW + pix0 + q] = from_f<T>(v);
+  }
+}
+
 template <typename T>
 __global__ void cast_from_f32_kernel(const float* __restrict__ src, T* __restrict__ dst, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -264,7 +412,124 @@ static int ac_bwd(const void* fmap1, const void* fmap2, int b, int n1, int n2, i
   return HS2_OK;
 }
 
+template <typename T>
+static int ac_pack(const void* fmap, int b, int n, int c, int h, int w, const int64_t* frames, int num_frames,
+                   void* packed, unsigned char* flags, cudaStream_t s) {
+  if (frames) {
+    HS2_CUDA(cudaMemsetAsync(flags, 0, (size_t)n, s));
+    if (num_frames > 0) {
+      altcorr_flag_kernel<<<(num_frames + 255) / 256, 256, 0, s>>>(frames, num_frames, n, flags);
+      HS2_LAUNCH_CHECK("altcorr_flag_kernel");
+    }
+  }
+  dim3 grid((h * w + 31) / 32, n, b);
+  HS2_PROF("altcorr_pack", s);
+  altcorr_pack_kernel<T><<<grid, kAcThreads, 0, s>>>(static_cast<const T*>(fmap), static_cast<T*>(packed),
+                                                     frames ? flags : nullptr, n, c, h * w);
+  HS2_LAUNCH_CHECK("altcorr_pack_kernel");
+  return HS2_OK;
+}
+
+template <typename T, int NCH>
+static int ac_fwd_packed_n(const void* p1, const void* p2, int b, int n1, int n2, int h, int w, int h2, int w2,
+                           const float* coords, const int64_t* ii, const int64_t* jj, int m, int radius, void* corr,
+                           int32_t* info, cudaStream_t s) {
+  const int stride = ac_stride(radius);
+  const size_t smem = (size_t)kAcPix * (stride * 4 + 16);
+  if (smem > 48 * 1024)
+    HS2_CUDA(cudaFuncSetAttribute(altcorr_fwd_packed_kernel<T, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+  dim3 grid((h * w + kAcPix - 1) / kAcPix, m, b);
+  HS2_PROF("altcorr_fwd_packed", s);
+  altcorr_fwd_packed_kernel<T, NCH><<<grid, kAcThreads, smem, s>>>(
+      static_cast<const T*>(p1), static_cast<const T*>(p2), coords, ii, jj, static_cast<T*>(corr), n1, n2, h, w, h2,
+      w2, m, radius, stride, info);
+  HS2_LAUNCH_CHECK("altcorr_fwd_packed_kernel");
+  return HS2_OK;
+}
+
+template <typename T>
+static int ac_fwd_packed(const void* p1, const void* p2, int b, int n1, int n2, int c, int h, int w, int h2, int w2,
+                         const float* coords, const int64_t* ii, const int64_t* jj, int m, int radius, void* corr,
+                         int32_t* info, cudaStream_t s) {
+  switch (c) {
+    case 32: return ac_fwd_packed_n<T, 1>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case 64: return ac_fwd_packed_n<T, 2>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case 128: return ac_fwd_packed_n<T, 4>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case 256: return ac_fwd_packed_n<T, 8>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+  }
+  set_error("altcorr_forward_packed: channels must be 32, 64, 128 or 256 (got %d)", c);
+  return HS2_ERR_INVALID;
+}
+
+static size_t ac_packed_bytes(int dtype, int b, int n, int c, int h, int w) {
+  return (size_t)b * n * h * w * c * (dtype == HS2_F16 || dtype == HS2_BF16 ? 2 : 0);
+}
+
 }  // namespace hs2
+
+extern "C" int hs2_altcorr_pack_workspace_size(int dtype, int b, int n, int c, int h, int w, size_t* bytes) {
+  using namespace hs2;
+  if (!bytes) {
+    set_error("altcorr_pack_workspace_size: null output");
+    return HS2_ERR_INVALID;
+  }
+  if (dtype != HS2_F16 && dtype != HS2_BF16) {
+    set_error("altcorr_pack: float16 or bfloat16 features only (dtype %d)", dtype);
+    return HS2_ERR_DTYPE;
+  }
+  if (b < 0 || n < 0 || c <= 0 || c > 256 || h <= 0 || w <= 0) {
+    set_error("altcorr_pack: bad sizes b=%d n=%d c=%d h=%d w=%d", b, n, c, h, w);
+    return HS2_ERR_INVALID;
+  }
+  *bytes = ((ac_packed_bytes(dtype, b, n, c, h, w) + 255) & ~(size_t)255) + (size_t)n + 256;
+  return HS2_OK;
+}
+
+extern "C" int hs2_altcorr_pack(const void* fmap, int dtype, int b, int n, int c, int h, int w,
+                                const int64_t* frames, int num_frames, void* workspace, size_t workspace_bytes,
+                                hs2_stream_t stream) {
+  using namespace hs2;
+  size_t need = 0;
+  int rc = hs2_altcorr_pack_workspace_size(dtype, b, n, c, h, w, &need);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < need) {
+    set_error("altcorr_pack: workspace of %zu bytes required", need);
+    return HS2_ERR_WORKSPACE;
+  }
+  if (num_frames < 0 || (num_frames > 0 && !frames)) {
+    set_error("altcorr_pack: bad frame list (%d)", num_frames);
+    return HS2_ERR_INVALID;
+  }
+  if (b == 0 || n == 0) return HS2_OK;
+  if ((rc = bind_device(workspace))) return rc;
+  unsigned char* flags = static_cast<unsigned char*>(workspace) +
+                         ((ac_packed_bytes(dtype, b, n, c, h, w) + 255) & ~(size_t)255);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == HS2_F16) return ac_pack<__half>(fmap, b, n, c, h, w, frames, num_frames, workspace, flags, s);
+  return ac_pack<__nv_bfloat16>(fmap, b, n, c, h, w, frames, num_frames, workspace, flags, s);
+}
+
+extern "C" int hs2_altcorr_forward_packed(const void* packed1, const void* packed2, int dtype, int b, int n1, int n2,
+                                          int c, int h, int w, int h2, int w2, const float* coords,
+                                          const int64_t* ii, const int64_t* jj, int m, int radius, void* corr,
+                                          int32_t* info, hs2_stream_t stream) {
+  using namespace hs2;
+  int rc = ac_check("altcorr_forward_packed", b, n1, n2, c, h, w, h2, w2, m, radius);
+  if (rc) return rc;
+  if (dtype != HS2_F16 && dtype != HS2_BF16) {
+    set_error("altcorr_forward_packed: float16 or bfloat16 features only (dtype %d)", dtype);
+    return HS2_ERR_DTYPE;
+  }
+  if (m == 0 || b == 0) return HS2_OK;
+  if ((rc = bind_device(corr))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == HS2_F16)
+    return ac_fwd_packed<__half>(packed1, packed2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr, info,
+                                 s);
+  return ac_fwd_packed<__nv_bfloat16>(packed1, packed2, b, n1, n2, c, h, w, h2, w2, coords, ii, jj, m, radius, corr,
+                                      info, s);
+}
 
 extern "C" int hs2_altcorr_forward(const void* fmap1, const void* fmap2, int dtype, int b, int n1, int n2,
                                    int c, int h, int w, int h2, int w2, const float* coords, const int64_t* ii,

@@ -681,8 +681,10 @@ constexpr int kTcThreads = 320;
 constexpr int kTcSplitWarps = 8;
 constexpr int kTcK = 32;                       // pixels per stage (128 B per plane row)
 constexpr int kTcMaxStages = 6;                // stages of frames of <= 128 tile rows
-constexpr int kTcSkip = 112;                   // Gram columns M tile 1 leaves out (< 6 * 21, 8-row aligned)
-constexpr int kTcMaxBlocks = 42;               // N <= 6*42 + 1 <= 256
+constexpr int kTcSkip = 112;                   // Gram columns M tile 1 leaves out (<= 126, 16-aligned)
+// Schur rows of D values per frame on the tensor cores: N = D * rows + 1 <= 256
+__host__ __device__ constexpr int tc_max_blocks(int D) { return 255 / D; }
+constexpr int kTcMaxBlocks = tc_max_blocks(6);  // 42 for the SE3 rows of ba
 constexpr int kTcRows = 256;                   // plane rows per tile
 constexpr int kTcBox = 64;                     // plane rows per TMA box
 constexpr int kTcTile = kTcRows * kTcK * 4;    // 32 KB
@@ -754,23 +756,24 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
   return (uint32_t)(r * 128 + ((((k >> 2) ^ (r & 7)) & 7) << 4) + ((k & 3) << 2));
 }
 
+template <int D>
 __global__ void __launch_bounds__(kTcThreads, 1)
-ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, BaPtrs w, int P,
+ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, BaPtrs w, int64_t lda,
                    int32_t* __restrict__ info, int split3) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int nr = w.sptr[s + 1] - w.sptr[s];
-  if (nr == 0 || nr > kTcMaxBlocks) return;
-  const int mtiles = (6 * nr + 127) / 128;          // 128-row M tiles, both in this CTA
+  if (nr == 0 || nr > tc_max_blocks(D)) return;
+  const int mtiles = (D * nr + 127) / 128;          // 128-row M tiles, both in this CTA
   const int c0 = blockIdx.z * chunk;
   const int c1 = min(HW, c0 + chunk);
   if (c0 >= c1) return;
-  const int nrowB = 6 * nr + 1;                   // + the sqrt(Q) w row
+  const int nrowB = D * nr + 1;                   // + the sqrt(Q) w row
   const int Npad = (nrowB + 15) & ~15;
-  const int nbox = (6 * nr + kTcBox - 1) / kTcBox;
+  const int nbox = (D * nr + kTcBox - 1) / kTcBox;
   const int nchunks = (c1 - c0 + kTcK - 1) / kTcK;
-  const int prow0 = w.rptr[s] * 6;                 // first plane row of the frame's Schur rows
+  const int prow0 = w.rptr[s] * D;                 // first plane row of the frame's Schur rows
 
   extern __shared__ uint8_t tc_raw[];
   const uint32_t raw = smem_u32(tc_raw);
@@ -846,8 +849,8 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
         for (int u = 0; u < 8; ++u) {
           const int r = rb + u * kTcSplitWarps;
           float v = 0.f;
-          if (r < 6 * nr) v = *reinterpret_cast<const float*>(hi + sw128_off(r, lane)) * sq;
-          else if (r == 6 * nr) v = wq;
+          if (r < D * nr) v = *reinterpret_cast<const float*>(hi + sw128_off(r, lane)) * sq;
+          else if (r == D * nr) v = wq;
           g[u] = v;
         }
 #pragma unroll
@@ -871,7 +874,7 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     }
   } else if (lane == 0) {
     // ------------------------------------------------------------- MMA issuer
-    // M tile 1 (rows >= 128) only needs the columns of blocks b >= a >= 21, i.e. from 126 on:
+    // M tile 1 (rows >= 128) only needs the columns of blocks b >= a >= 128 / D, i.e. from 126 on:
     // its B operand starts at row kTcSkip (a multiple of 8 rows, N stays a multiple of 16)
     const uint32_t idesc0 = umma_idesc_tf32(128, Npad), idesc1 = umma_idesc_tf32(128, Npad - kTcSkip);
     for (int c = 0; c < nchunks; ++c) {
@@ -906,11 +909,11 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
     const bool ok = mbar_wait(bar_done, 0, abort_flag);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int quarter = warp & 3;                    // TMEM lane quarter of this warp
-    const int64_t n = 6 * (int64_t)P;
+    const int64_t n = lda;
     for (int mt = 0; mt < mtiles; ++mt) {
       const int R = mt * 128 + quarter * 32 + lane;  // plane row of this accumulator row
-      const bool mrow = ok && R < 6 * nr;
-      const int a = R / 6, x = R % 6;
+      const bool mrow = ok && R < D * nr;
+      const int a = R / D, x = R % D;
       const int pa = mrow ? spose[a] : 0;
       const int cbase = mt ? kTcSkip : 0;             // first Gram column held by this M tile
       for (int col0 = (warp >> 2) * 16; cbase + col0 < Npad; col0 += 32) {
@@ -927,18 +930,18 @@ ba_schur_tc_kernel(const __grid_constant__ CUtensorMap emap, int HW, int chunk, 
         for (int j = 0; j < 16; ++j) {
           const int col = cbase + col0 + j;
           const double val = -(double)__uint_as_float(v[j]);
-          if (col < 6 * nr) {
-            const int b = col / 6, y = col % 6;
+          if (col < D * nr) {
+            const int b = col / D, y = col % D;
             if (b < a) continue;
             const int pb = spose[b];
-            if (pa > pb) atomicAdd(&w.A[(pa * 6 + x) * n + pb * 6 + y], val);
-            else if (pa < pb) atomicAdd(&w.A[(pb * 6 + y) * n + pa * 6 + x], val);
+            if (pa > pb) atomicAdd(&w.A[(pa * D + x) * n + pb * D + y], val);
+            else if (pa < pb) atomicAdd(&w.A[(pb * D + y) * n + pa * D + x], val);
             else {
-              atomicAdd(&w.A[(pa * 6 + x) * n + pa * 6 + y], val);
-              if (a != b) atomicAdd(&w.A[(pa * 6 + y) * n + pa * 6 + x], val);
+              atomicAdd(&w.A[(pa * D + x) * n + pa * D + y], val);
+              if (a != b) atomicAdd(&w.A[(pa * D + y) * n + pa * D + x], val);
             }
-          } else if (col == 6 * nr) {
-            atomicAdd(&w.b[pa * 6 + x], val);
+          } else if (col == D * nr) {
+            atomicAdd(&w.b[pa * D + x], val);
           }
         }
       }
@@ -1348,7 +1351,8 @@ static int encode_erows_map(CUtensorMap* map, float* erows, int HW, int64_t plan
 //         slices), in parallel with the remaining tiles of update kb
 //         (column blocks kb+2 ..) on the other CTAs                         | barrier
 //   backward  x_c = L_cc^-T (y_c - sum_{j>c} L_jc^T x_j), one CTA per block c,
-//             ordered by per-block ready flags instead of grid barriers
+//             ordered by per-block ready flags instead of grid barriers; L_cc^-1
+//             formed in shared memory while the blocks above are solved
 //
 // Panel kb, task t: the CTA holds [D; X | b] in shared memory (D the 64x64 diagonal
 // block, redundantly in every CTA of the panel; X the t-th 64-row tile below D, none
@@ -1752,41 +1756,58 @@ __device__ bool chol_panel(int n, int kb, int t, double* __restrict__ A, double*
   return true;
 }
 
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // A[ri + i][rj + j] -= sum_k L[ri + i][o + k] L[rj + j][o + k] over the 16*RG rows
 // at ri and the 64 columns at rj; `diag` keeps only entries on or below the
-// diagonal of A.  Thread (ty, tx) owns rows ty + 16a and columns tx + 16c.
+// diagonal of A.  Thread (ty, tx) owns rows ty + 16a and columns tx + 16c.  Both L row
+// blocks and the target tile itself arrive by 16-byte cp.async copies issued together
+// (one L2 round trip; rows and columns outside the matrix are zero-filled).
 template <int RG>
 __device__ void chol_update_tile(int n, double* __restrict__ A, int o, int ri, int rj, bool diag, double* csm) {
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   const int ni = min(16 * RG, n - ri), nj = min(kNB, n - rj);
   if (ni <= 0) return;
+  constexpr int kRows = 16 * RG;
   double (*Ai)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);
   double (*Aj)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm + 64 * kPLD);
+  double (*Cs)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm + 128 * kPLD);
   __syncthreads();
   {
-    double2 va[RG * 2], vb[8];
-#pragma unroll
-    for (int q = 0; q < RG * 2; ++q) {
-      const int idx = tid + q * kCholThreads;   // double2 index in the (16 RG) x 32 grid
-      const int a = idx >> 5, k = (idx & 31) * 2;
-      va[q] = a < ni ? ldcg2(&A[(int64_t)(ri + a) * n + o + k]) : make_double2(0.0, 0.0);
+    const uint32_t sb = smem_u32(csm);
+    for (int idx = tid; idx < (2 * kRows + 64) * 32; idx += kCholThreads) {
+      const int r = idx >> 5, k = (idx & 31) * 2;
+      int srow, a;
+      int64_t grow;
+      int gcol;
+      bool live;
+      if (r < kRows) {                       // L rows of the tile's block rows
+        srow = r;
+        live = r < ni;
+        grow = ri + r;
+        gcol = o + k;
+      } else if (r < kRows + 64) {           // L rows of the tile's block columns
+        a = r - kRows;
+        srow = 64 + a;
+        live = a < nj;
+        grow = rj + a;
+        gcol = o + k;
+      } else {                               // the tile
+        a = r - kRows - 64;
+        srow = 128 + a;
+        live = a < ni && k < nj;
+        grow = ri + a;
+        gcol = rj + k;
+      }
+      cp_async16(sb + (uint32_t)(srow * kPLD + k) * 8u, live ? (const void*)(A + grow * n + gcol) : (const void*)A,
+                 live ? 16u : 0u);
     }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int idx = tid + q * kCholThreads;
-      const int a = idx >> 5, k = (idx & 31) * 2;
-      vb[q] = a < nj ? ldcg2(&A[(int64_t)(rj + a) * n + o + k]) : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int q = 0; q < RG * 2; ++q) {
-      const int idx = tid + q * kCholThreads;
-      *reinterpret_cast<double2*>(&Ai[idx >> 5][(idx & 31) * 2]) = va[q];
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int idx = tid + q * kCholThreads;
-      *reinterpret_cast<double2*>(&Aj[idx >> 5][(idx & 31) * 2]) = vb[q];
-    }
+    cp_async_wait_all();
   }
   __syncthreads();
   double acc[RG][4];
@@ -1814,28 +1835,33 @@ __device__ void chol_update_tile(int n, double* __restrict__ A, int o, int ri, i
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const int i = ty + 16 * a, j = tx + 16 * c;
-      if (i < ni && j < nj && (!diag || rj + j <= ri + i)) {
-        double* dst = &A[(int64_t)(ri + i) * n + rj + j];
-        *dst = __ldcg(dst) - acc[a][c];
-      }
+      if (i < ni && j < nj && (!diag || rj + j <= ri + i)) A[(int64_t)(ri + i) * n + rj + j] = Cs[i][j] - acc[a][c];
     }
 }
 
 // Backward substitution L^T x = y, block c on CTA c mod G (blocks taken from the
-// highest down).  The CTA folds L_jc^T x_j into per-thread partial sums as the ready
-// flags of blocks j > c arrive (its loads of L_jc are issued before it waits), then
-// one warp solves with L_cc^T in registers and the block's flag is released.
+// highest down).  The CTA first inverts L_cc in shared memory (row by row,
+// X_ij = -(1/L_ii) sum_{k=j}^{i-1} L_ik X_kj, column j on four threads each summing every
+// fourth k) -- for every block but the highest this overlaps the wait for the blocks
+// above -- then folds L_jc^T x_j into per-thread partial sums as the ready flags of
+// blocks j > c arrive (its loads of L_jc are issued before it waits), and forms
+// x_c = L_cc^-T (y_c - sum_j L_jc^T x_j) as one mat-vec: no 64-step dependency chain
+// sits between two ready flags.
 __device__ bool chol_backward(int n, int nbk, const double* __restrict__ A, CholBuf cb, double* __restrict__ x,
                               float* __restrict__ dx_out, int32_t* __restrict__ info, double* csm) {
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x;
   const int G = (int)gridDim.x, cta = (int)blockIdx.x;
   if (cta >= nbk) return true;
-  double (*Ls)[kNB] = reinterpret_cast<double (*)[kNB]>(csm);   // [64][64]
-  double* ys = csm + kNB * kNB;                                   // [64]
-  double* dv = ys + kNB;                                          // [64]
-  double* part = dv + kNB;                                        // [4][64]
+  constexpr unsigned kFull = 0xffffffffu;
+  double (*Ls)[kNB] = reinterpret_cast<double (*)[kNB]>(csm);              // [64][64] L_cc
+  double (*Li)[kNB] = reinterpret_cast<double (*)[kNB]>(csm + kNB * kNB);  // [64][64] L_cc^-1
+  double* ys = csm + 2 * kNB * kNB;                                         // [64]
+  double* dv = ys + kNB;                                                    // [64] 1/L_ii
+  double* part = dv + kNB;                                                  // [4][64]
+  double* rv = part + 4 * kNB;                                              // [64]
   __shared__ int s_abort;
   const int cl = tid & 63, rg = tid >> 6;
+  const int ic = tid >> 2, is = tid & 3;   // inversion: column ic, k phase is
   for (int c = cta + ((nbk - 1 - cta) / G) * G; c >= 0; c -= G) {
     const int oc = c * kNB, nc = min(kNB, n - oc);
     __syncthreads();
@@ -1848,6 +1874,28 @@ __device__ bool chol_backward(int n, int nbk, const double* __restrict__ A, Chol
     if (tid < kNB) {
       ys[tid] = tid < nc ? __ldcg(&cb.y[oc + tid]) : 0.0;
       dv[tid] = tid < nc ? __ldcg(&cb.dinv[(int64_t)c * kNB + tid]) : 0.0;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kNB * kNB; idx += kCholThreads) {
+      const int i = idx >> 6, l = idx & 63;
+      Li[i][l] = i == l ? dv[i] : 0.0;
+    }
+    __syncthreads();
+    for (int i = 1; i < nc; ++i) {
+      double p0 = 0.0, p1 = 0.0;
+      if (ic < i) {
+        int k = ic + is;
+        for (; k + 4 < i; k += 8) {
+          p0 = fma(Ls[i][k], Li[k][ic], p0);
+          p1 = fma(Ls[i][k + 4], Li[k + 4][ic], p1);
+        }
+        if (k < i) p0 = fma(Ls[i][k], Li[k][ic], p0);
+      }
+      double pv = p0 + p1;
+      pv += __shfl_xor_sync(kFull, pv, 1);
+      pv += __shfl_xor_sync(kFull, pv, 2);
+      if (ic < i && is == 0) Li[i][ic] = -dv[i] * pv;
+      __syncthreads();
     }
     double acc = 0.0;
     for (int j = nbk - 1; j > c; --j) {
@@ -1870,30 +1918,23 @@ __device__ bool chol_backward(int n, int nbk, const double* __restrict__ A, Chol
     }
     part[rg * kNB + cl] = acc;
     __syncthreads();
-    if (tid < 32) {
-      const unsigned kFull = 0xffffffffu;
-      double y0 = ys[lane] - ((part[lane] + part[kNB + lane]) + (part[2 * kNB + lane] + part[3 * kNB + lane]));
-      const int l1 = lane + 32;
-      double y1 = ys[l1] - ((part[l1] + part[kNB + l1]) + (part[2 * kNB + l1] + part[3 * kNB + l1]));
+    if (tid < kNB) rv[tid] = ys[tid] - ((part[tid] + part[kNB + tid]) + (part[2 * kNB + tid] + part[3 * kNB + tid]));
+    __syncthreads();
+    // x_i = sum_{k >= i} Li[k][i] r_k: output cl, rows k of quarter rg
+    {
+      double v = 0.0;
 #pragma unroll
-      for (int j = kNB - 1; j >= 0; --j) {
-        const double xj = __shfl_sync(kFull, j >= 32 ? y1 : y0, j & 31) * dv[j];
-        if (j >= 32) {
-          if (lane == j - 32) y1 = xj;
-        } else if (lane == j) {
-          y0 = xj;
-        }
-        if (lane < j) y0 = fma(-Ls[j][lane], xj, y0);
-        if (l1 < j) y1 = fma(-Ls[j][l1], xj, y1);
+      for (int r = 0; r < 16; ++r) {
+        const int k = rg * 16 + r;
+        if (k >= cl) v = fma(Li[k][cl], rv[k], v);
       }
-      if (lane < nc) {
-        x[oc + lane] = y0;
-        dx_out[oc + lane] = (float)y0;
-      }
-      if (l1 < nc) {
-        x[oc + l1] = y1;
-        dx_out[oc + l1] = (float)y1;
-      }
+      part[rg * kNB + cl] = v;
+    }
+    __syncthreads();
+    if (tid < nc) {
+      const double xv = (part[tid] + part[kNB + tid]) + (part[2 * kNB + tid] + part[3 * kNB + tid]);
+      x[oc + tid] = xv;
+      dx_out[oc + tid] = (float)xv;
     }
     __syncthreads();
     if (tid == 0) st_release_gpu(cb.ctl + kCtlFlags + c, 1u);
@@ -2130,7 +2171,8 @@ static int run_cholesky(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* 
   if (n == 0) return HS2_OK;
   HS2_PROF("ba_cholesky", s);
   const int nbk = (n + kNB - 1) / kNB;
-  const size_t smem = sizeof(double) * (128 * kPLD + 128 + 64 + 72 + 2);   // panel (tile, backward need less)
+  // panel: [128][kPLD] + b, 1/L_jj, exchange; tile: [192][kPLD]; backward: 2 x 64 x 64 + 256
+  const size_t smem = sizeof(double) * std::max<size_t>(128 * kPLD + 128 + 64 + 72 + 2, 192 * kPLD);
   static DeviceOnce once;
   static std::atomic<int> grid_cap[kMaxDevices];
   int dev = 0;
@@ -2253,7 +2295,7 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
       int dev = 0;
       HS2_CUDA(cudaGetDevice(&dev));
       int rc = once.run(dev, [&]() -> int {
-        HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
         return HS2_OK;
       });
       if (rc) return rc;
@@ -2261,7 +2303,8 @@ static int build_system(const BaProblem& p, const BaLaunch& l, const float* pose
       rc = encode_erows_map(&emap, w.erows, p.HW, 6 * ((int64_t)P + p.E));
       if (rc) return rc;
       dim3 grid((unsigned)S, 1u, l.tc_split);
-      ba_schur_tc_kernel<<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, P, info, g_gram_split3.load());
+      ba_schur_tc_kernel<6><<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, w, n, info,
+                                                              g_gram_split3.load());
       HS2_LAUNCH_CHECK("ba_schur_tc_kernel");
     }
     dim3 grid((unsigned)S, l.schur_split);
@@ -3077,11 +3120,12 @@ constexpr int kPgGThreads = 64;
 
 __global__ void __launch_bounds__(kPgGThreads)
 pg_schur_kernel(int HW, int64_t npad, BaPtrs w, const float* __restrict__ erows, const float* __restrict__ qbuf,
-                double* __restrict__ A, const int32_t* __restrict__ info) {
+                double* __restrict__ A, int min_rows, const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int r0 = w.sptr[s], nr = w.sptr[s + 1] - r0;
+  if (nr < min_rows) return;   // frames of fewer Schur rows run on the tensor-core Gram
   const int64_t rbase = w.rptr[s];   // storage position of the frame's first Schur row
   const int m = kPgD * nr, nt = (m + kPgGT - 1) / kPgGT, T = nt * (nt + 1) / 2;
   const int64_t HWs = row_stride(HW);
@@ -3149,11 +3193,13 @@ pg_schur_kernel(int HW, int64_t npad, BaPtrs w, const float* __restrict__ erows,
 // b -= E.(Q w) for every Schur row (Ev6x1 :1525-1560); one warp per (row, plane).
 __global__ void __launch_bounds__(256)
 pg_schur_rhs_kernel(int HW, BaPtrs w, const float* __restrict__ erows, const float* __restrict__ qbuf,
-                    const float* __restrict__ wbuf, double* __restrict__ b, const int32_t* __restrict__ info) {
+                    const float* __restrict__ wbuf, double* __restrict__ b, int min_rows,
+                    const int32_t* __restrict__ info) {
   if (info[0]) return;
   const int s = blockIdx.x;
   if (s >= info[1]) return;
   const int r0 = w.sptr[s], nr = w.sptr[s + 1] - r0;
+  if (nr < min_rows) return;
   const size_t HWs = (size_t)row_stride(HW);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float* Q = qbuf + (int64_t)s * HW;
@@ -3345,9 +3391,35 @@ extern "C" int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int
   }
   if (P > 0 && S > 0) {
     HS2_PROF("pg_schur", s);
-    pg_schur_kernel<<<dim3((unsigned)S, kPgSplit), kPgGThreads, 0, s>>>(p.HW, npad, w, erows, qbuf, w.A, info);
+    // frames of <= 36 Schur rows (N = 7 R + 1 <= 256): the tensor-core Gram of ba with
+    // 7-value rows, its w row giving the rhs; larger frames: the SIMT Gram + rhs kernels
+    const bool tc = g_schur_path.load() == 0;
+    if (tc) {
+      static DeviceOnce once;
+      int dev = 0;
+      HS2_CUDA(cudaGetDevice(&dev));
+      rc = once.run(dev, [&]() -> int {
+        HS2_CUDA(cudaFuncSetAttribute(ba_schur_tc_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        return HS2_OK;
+      });
+      if (rc) return rc;
+      CUtensorMap emap;
+      if ((rc = encode_erows_map(&emap, erows, p.HW, kPgD * ((int64_t)P + E)))) return rc;
+      BaPtrs wt = w;
+      wt.erows = erows;
+      wt.qbuf = qbuf;
+      wt.wbuf = wbuf;
+      const BaLaunch l = ba_launch_shape(p);
+      dim3 grid((unsigned)S, 1u, l.tc_split);
+      ba_schur_tc_kernel<7><<<grid, kTcThreads, kTcSmem, s>>>(emap, p.HW, l.tc_chunk, wt, npad, info,
+                                                              g_gram_split3.load());
+      HS2_LAUNCH_CHECK("ba_schur_tc_kernel<7>");
+    }
+    const int min_rows = tc ? tc_max_blocks(kPgD) + 1 : 0;
+    pg_schur_kernel<<<dim3((unsigned)S, kPgSplit), kPgGThreads, 0, s>>>(p.HW, npad, w, erows, qbuf, w.A, min_rows,
+                                                                        info);
     HS2_LAUNCH_CHECK("pg_schur_kernel");
-    pg_schur_rhs_kernel<<<(unsigned)S, 256, 0, s>>>(p.HW, w, erows, qbuf, wbuf, w.b, info);
+    pg_schur_rhs_kernel<<<(unsigned)S, 256, 0, s>>>(p.HW, w, erows, qbuf, wbuf, w.b, min_rows, info);
     HS2_LAUNCH_CHECK("pg_schur_rhs_kernel");
   }
   if (P > 0) {

@@ -206,6 +206,25 @@ int hs2_altcorr_forward(const void* fmap1, const void* fmap2, int dtype, int b, 
                         const int64_t* jj, int m, int radius, void* corr, int32_t* info,
                         hs2_stream_t stream);
 
+/* altcorr_forward on channel-last features (same reference op; float16 / bfloat16 with
+ * c in {32, 64, 128, 256}).  hs2_altcorr_pack writes fmap [b,n,c,h,w] channel-last,
+ * [b,n,h*w,c], into the start of `workspace` (hs2_altcorr_pack_workspace_size() bytes,
+ * a frame-flag array at its end): only the frames listed in `frames[num_frames]` (the
+ * ii or jj of a call), or all n frames when `frames` is null.  hs2_altcorr_forward_packed
+ * then takes two such buffers in place of fmap1 / fmap2 and writes the same corr as
+ * hs2_altcorr_forward: products of the 16-bit features formed exactly and summed in
+ * FP32 (the reference rounds each product to the feature type first), window rows read
+ * as contiguous channel vectors.  A caller that looks up many edge chunks against one
+ * pyramid (AltCorrBlock) packs each level once.
+ */
+int hs2_altcorr_pack_workspace_size(int dtype, int b, int n, int c, int h, int w, size_t* bytes);
+int hs2_altcorr_pack(const void* fmap, int dtype, int b, int n, int c, int h, int w, const int64_t* frames,
+                     int num_frames, void* workspace, size_t workspace_bytes, hs2_stream_t stream);
+int hs2_altcorr_forward_packed(const void* packed1, const void* packed2, int dtype, int b, int n1, int n2, int c,
+                               int h, int w, int h2, int w2, const float* coords, const int64_t* ii,
+                               const int64_t* jj, int m, int radius, void* corr, int32_t* info,
+                               hs2_stream_t stream);
+
 /* altcorr_backward  (reference: src/droid.cpp:291-305, src/altcorr_kernel.cu:79-129,175-225;
  *   effective positional order as called from hislam2/modules/corr.py:86)
  *   grad [b,m,2r+1,2r+1,h,w] f32 (same layout as the forward output).

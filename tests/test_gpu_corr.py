@@ -160,3 +160,65 @@ def test_altcorr_bad_index_zero_filled(cuda):
     ii[1] = 7
     out, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, 2)
     assert torch.count_nonzero(out[:, 1]) == 0
+
+
+def make_alt_levels(B, N1, N2, C, H, W, level, M, seed, dev, dtype):
+    """fmap1 at H x W, fmap2 at level `level` (H >> level, W >> level), coords at that level's
+    scale spread past the borders, ii/jj over the frames (one edge index out of range
+    is not included here)."""
+    g = torch.Generator().manual_seed(seed)
+    H2, W2 = H >> level, W >> level
+    f1 = (torch.randn(B, N1, C, H, W, generator=g) / np.sqrt(C)).to(dev, dtype)
+    f2 = (torch.randn(B, N2, C, H2, W2, generator=g) / np.sqrt(C)).to(dev, dtype)
+    ii = torch.randint(0, N1, (M,), generator=g).to(dev)
+    jj = torch.randint(0, N2, (M,), generator=g).to(dev)
+    crd = torch.stack([-3 + (W2 + 6) * torch.rand(B, M, H, W, generator=g),
+                       -3 + (H2 + 6) * torch.rand(B, M, H, W, generator=g)], 2)
+    return f1, f2, crd.to(dev).contiguous(), ii, jj
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16], ids=["f16", "bf16"])
+@pytest.mark.parametrize("C,r,level", [(128, 3, 0), (128, 3, 2), (128, 4, 1), (32, 3, 0), (64, 2, 3), (256, 3, 1)])
+def test_altcorr_packed_vs_oracle(cuda, dtype, C, r, level):
+    """The channel-last path (exact products, FP32 sums) against the float64 oracle on
+    the same 16-bit inputs: only the rounding of the stored output differs (2^-10
+    relative for float16, 2^-7 for bfloat16), and against the direct kernel."""
+    f1, f2, crd, ii, jj = make_alt_levels(1, 3, 5, C, 24, 40, level, 6, seed=C + r + level, dev=cuda, dtype=dtype)
+    out, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, r)
+    direct, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, r, path="direct")
+    ref = oc.altcorr_forward(np64(f1), np64(f2), np64(crd), ii.cpu().numpy(), jj.cpu().numpy(), r)
+    tol = 2 ** -10 if dtype == torch.float16 else 2 ** -7
+    assert tuple(out.shape) == ref.shape
+    assert rel(np64(out), ref) < tol
+    assert rel(np64(out), np64(direct)) < tol
+
+
+def test_altcorr_packed_frame_subsets_and_bad_index(cuda):
+    """Only the frames of ii / jj are packed; an edge whose frame is out of range is
+    zero-filled and reported, like the direct kernel."""
+    f1, f2, crd, ii, jj = make_alt_levels(2, 6, 6, 128, 16, 24, 0, 4, seed=3, dev=cuda, dtype=torch.float16)
+    ii = torch.tensor([5, 0, 5, 9], device=cuda)
+    out, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, 3)
+    good = [0, 1, 2]
+    ref = oc.altcorr_forward(np64(f1), np64(f2), np64(crd[:, good]), ii[good].cpu().numpy(),
+                             jj[good].cpu().numpy(), 3)
+    assert rel(np64(out[:, good]), ref) < 2 ** -10
+    assert torch.count_nonzero(out[:, 3]) == 0
+
+
+def test_altcorr_packed_frontend_size(cuda):
+    """43x77, 128 channels, radius 3, the four pooled levels of AltCorrBlock: the packed
+    block (pyramid packed once) against CorrLayer on the direct kernel."""
+    from hislam2_b200 import corr as hcorr
+    c = synth.make_corr_problem("frontend", seed=2, device=cuda, num_edges=24, dtype=torch.float16)
+    f = c["fmaps"][None].contiguous()
+    coords = c["coords"][None].contiguous()
+    blk = hcorr.AltCorrBlock(f, num_levels=4, radius=3)
+    assert blk.packed is not None
+    with torch.no_grad():
+        fast = blk(coords, c["ii"], c["jj"])
+    blk.packed = None
+    with torch.no_grad():
+        slow = blk(coords, c["ii"], c["jj"])
+    assert fast.shape == slow.shape == (1, 24, 4 * 49, 43, 77)
+    assert rel(np64(fast), np64(slow)) < 2 ** -10
