@@ -297,6 +297,7 @@ def run_ours(args, world, rank, local):
     corr = corr_lookup(args, dev, world, peaks)
     pg = pgba_leg(args, dev, world, rank)
     alt = altcorr_leg(args, dev, world, peaks)
+    step = backend_step_leg(args, dev, world)
     vol = volume_leg(args, dev, world, peaks) if world == 1 else None
     bat = batch_leg(args, dev, world, rank)
 
@@ -317,7 +318,7 @@ def run_ours(args, world, rank, local):
                 "config": dict(CONFIG, parallelism="replicas: one independent window per rank" if world > 1 else
                                "single GPU"),
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "accuracy": acc, "corr_lookup": corr, "altcorr": alt, "corr_volume": vol, "batch": bat, "pgba": pg, "clocks": clk,
+                "accuracy": acc, "corr_lookup": corr, "altcorr": alt, "backend_step": step, "corr_volume": vol, "batch": bat, "pgba": pg, "clocks": clk,
                 "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
                 "library_peaks_tflops": {"sgemm_fp32": round(simt[0], 2), "dgemm_fp64": round(simt[1], 2)}}
         print(json.dumps(line), flush=True)
@@ -383,7 +384,8 @@ def corr_lookup(args, dev, world, peaks):
     return {"value": round(gbs, 2), "unit": "GB/s", "ms_per_lookup": round(ms, 4),
             "config": "258 edges (frontend window), 43x77, 4 levels, radius 4, fp16 volumes",
             "roofline": {"bound": "hbm", "achieved": round(gbs / world, 2), "peak": peaks["hbm_gbs"],
-                         "unit": "GB/s", "frac": round(gbs / world / peaks["hbm_gbs"], 4)}}
+                         "unit": "GB/s", "frac": round(gbs / world / peaks["hbm_gbs"], 4),
+                         "peak_source": peaks["source"]}}
 
 
 def volume_leg(args, dev, world, peaks):
@@ -421,7 +423,8 @@ def volume_leg(args, dev, world, peaks):
         res["speedup_vs_torch_f16"] = round(ms_t / res["f16"]["ms"], 2)
         res["roofline"] = {"bound": "hbm", "achieved": round((out_bytes + in_bytes) / (res["f16"]["kernel_ms"] / 1e3)
                                                              / 1e9, 1),
-                           "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": res["f16"]["hbm_frac"]}
+                           "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": res["f16"]["hbm_frac"],
+                           "peak_source": peaks["source"]}
     torch.cuda.empty_cache()
     return res
 
@@ -532,6 +535,89 @@ def altcorr_leg(args, dev, world, peaks):
            "tflops_fp32_simt": round(flops / (ms / 1e3) / 1e12, 2), "write_gbs": round(out_bytes / (ms / 1e3) / 1e9, 1),
            "algorithmic": {"gflop": round(flops / 1e9, 1), "write_gb": round(out_bytes / 1e9, 3)}}
     del pyr, chunks
+    torch.cuda.empty_cache()
+    return res
+
+
+def backend_step_leg(args, dev, world):
+    """One update step of HI-SLAM2's backend global BA on the 300-keyframe window
+    (factor_graph.py:240-277: the radius-3, 4-level correlation of all 6000 edges in
+    chunks of two source frames, then cuda_ba with itrs = 2 GN iterations), timed three
+    ways on the device (the update network between them is out of scope):
+      plain_fp32   float32 features, the direct altcorr kernel (the reference's method:
+                   one dot product per window tap), BA in the FP32 form (3xTF32 Gram);
+      fp16_packed  float16 features (the reference runtime's dtype) through AltCorrBlock's
+                   channel-last path, same BA;
+      mixed_tc     bfloat16 features, per chunk the tcgen05 volume pyramid (corr_volume)
+                   and the radius-3 lookup (corr_index_forward), BA with the one-product
+                   TF32 Gram (its pose error vs FP64 is the `accuracy` entry's mixed form).
+    value = GN iterations per second of the whole step (2 / step time)."""
+    import droid_backends
+    from hislam2_b200 import _lib, backends, synth
+    from hislam2_b200.corr import AltCorrBlock, _pool_pyramid
+    p = synth.make_ba_problem(WORKLOAD, seed=0, device=dev)
+    g = torch.Generator().manual_seed(17)
+    K, H, W, C, r, L, itrs = 300, 43, 77, 128, 3, 4, 2
+    f32 = (torch.randn(K, C, H, W, generator=g) / np.sqrt(C)).to(dev)
+    ii, jj = p["ii"], p["jj"]
+    coords = synth.reproject(p["poses_gt"].cpu(), p["disps_gt"].cpu(), p["intrinsics"].cpu(), ii.cpu(), jj.cpu())
+    coords = (coords.float() + torch.randn(coords.shape, generator=g)).to(dev)           # [E, H, W, 2]
+    chunks = []
+    for i in range(0, int(jj.max()) + 1, 2):
+        v = ((ii >= i) & (ii < i + 2)).nonzero().flatten()
+        if v.numel():
+            crd = coords[v][None].contiguous()
+            c5 = crd.permute(0, 1, 4, 2, 3).contiguous()
+            chunks.append((ii[v].contiguous(), jj[v].contiguous(), crd,
+                           [(c5 / 2 ** lvl).contiguous() for lvl in range(L)]))
+    init_poses, init_disps = p["poses"].clone(), p["disps"].clone()
+    poses, disps = init_poses.clone(), init_disps.clone()
+
+    def ba():
+        poses.copy_(init_poses)
+        disps.copy_(init_disps)
+        droid_backends.ba(poses, disps, p["intrinsics"], p["targets"], p["weights"], p["eta"], p["ii"], p["jj"],
+                          p["t0"], p["t1"], itrs, p["lm"], p["ep"], False)
+
+    pyr32 = [lv[None].contiguous() for lv in _pool_pyramid(f32, L)]
+
+    def plain():
+        for ci, cj, _, crd in chunks:
+            for lvl in range(L):
+                backends.altcorr_forward(pyr32[0], pyr32[lvl], crd[lvl], ci, cj, r, path="direct")
+        ba()
+
+    blk = AltCorrBlock(f32.half()[None].contiguous(), num_levels=L, radius=r)
+
+    def fp16_packed():
+        with torch.no_grad():
+            for ci, cj, crd, _ in chunks:
+                blk(crd, ci, cj)
+        ba()
+
+    fbf = f32.bfloat16().contiguous()
+
+    def mixed_tc():
+        for ci, cj, _, crd in chunks:
+            levels = backends.corr_volume(fbf, fbf, ci, cj, num_levels=L)
+            for lvl in range(L):
+                droid_backends.corr_index_forward(levels[lvl], crd[lvl][0], r)
+        _lib.set_gram_precision(0)
+        try:
+            ba()
+        finally:
+            _lib.set_gram_precision(1)
+
+    res = {"config": "300 keyframes, 6000 edges in %d chunks, 43x77, 128 channels, radius 3, 4 levels, "
+                     "itrs = 2 GN iterations per step" % len(chunks), "unit": "GN iters/s"}
+    barrier(world)
+    for name, fn, n in (("plain_fp32", plain, 1), ("fp16_packed", fp16_packed, 2), ("mixed_tc", mixed_tc, 2)):
+        ms = max_over_ranks(device_time(fn, n, warmup=1), world, dev)
+        res[name] = {"ms_per_step": round(ms, 2), "gn_iters_per_s": round(itrs * 1e3 / ms * world, 3)}
+        torch.cuda.empty_cache()
+    for name in ("fp16_packed", "mixed_tc"):
+        res[name]["vs_plain"] = round(res[name]["gn_iters_per_s"] / res["plain_fp32"]["gn_iters_per_s"], 2)
+    del blk, pyr32, chunks
     torch.cuda.empty_cache()
     return res
 
@@ -793,7 +879,26 @@ def profile_batch(args, dev):
     plan.run(args.profile_iters)
 
 
-PROFILE_CASES = {"ba": profile_ba, "volume": profile_volume, "adjoint": profile_adjoint, "batch": profile_batch}
+def profile_altcorr(args, dev):
+    """AltCorrBlock (float16, radius 3, 4 levels, pyramid packed channel-last) on the
+    first --profile-edges edges of the 300-keyframe window: 4 altcorr_fwd_packed launches."""
+    from hislam2_b200 import synth
+    from hislam2_b200.corr import AltCorrBlock
+    p = synth.make_ba_problem(WORKLOAD, seed=0)
+    g = torch.Generator().manual_seed(17)
+    f = (torch.randn(1, 300, 128, 43, 77, generator=g) / np.sqrt(128)).half().to(dev)
+    E = min(args.profile_edges, p["ii"].numel())
+    ii, jj = p["ii"][:E].to(dev), p["jj"][:E].to(dev)
+    crd = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], p["ii"][:E], p["jj"][:E]).float()
+    crd = (crd + torch.randn(crd.shape, generator=g))[None].contiguous().to(dev)
+    blk = AltCorrBlock(f, num_levels=4, radius=3)
+    with torch.no_grad():
+        for _ in range(args.profile_iters):
+            blk(crd, ii, jj)
+
+
+PROFILE_CASES = {"ba": profile_ba, "volume": profile_volume, "adjoint": profile_adjoint, "batch": profile_batch,
+                 "altcorr": profile_altcorr}
 
 
 def main():

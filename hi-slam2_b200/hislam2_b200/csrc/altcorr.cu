@@ -336,6 +336,217 @@ altcorr_fwd_packed_kernel(const T* __restrict__ p1, const T* __restrict__ p2, co
   }
 }
 
+// ------------------------------------------------------------ tile forward ---
+// Dense local correlation on the tensor cores for C = 128 channels.  A CTA owns an 8x8
+// block of pixels of one edge.  The union of the block's D x D windows is a box of
+// bw x bh target positions (about 19 x 19 at 43x77 for reprojected coordinates); when it
+// holds at most kAtMaxPos positions the CTA stages the 64 source rows and the box's
+// rows (channel-last, 16-byte cp.async) in shared memory and computes the full
+// 64 x (bw bh) product with mma.sync m16n8k16 (16-bit operands, FP32 accumulation:
+// exact products, FP32 sums), then every output tap reads its four window values from
+// that product.  The product is 5-6x the taps actually needed, but it runs on the
+// tensor pipe and every target row is read once per block instead of once per pixel
+// and window row.  Blocks whose box is larger (coordinates scattered across the image)
+// fall back to the warp-per-pixel channel-last computation, so any input is correct.
+// mma.sync rather than tcgen05: the B operand is a data-dependent gathered box of
+// up to 384 rows and M is 64 (tcgen05 wants M = 128, i.e. a 16x8 block whose box no
+// longer fits next to its accumulator staging), and the kernel is bounded by the
+// staging and the gather epilogue, not by the tensor pipe.
+constexpr int kAtSide = 8;
+constexpr int kAtPix = kAtSide * kAtSide;
+constexpr int kAtMaxPos = 384;
+constexpr int kAtLd = 136;             // halves per staged row: 128 channels + 16 bytes of padding
+constexpr int kAtDLd = kAtMaxPos + 4;  // floats per row of the staged product
+constexpr size_t kAtSmem = (size_t)kAtPix * kAtLd * 2 + (size_t)kAtMaxPos * kAtLd * 2 +
+                           (size_t)kAtPix * kAtDLd * 4 + kAtPix * 16 + 64;
+
+template <typename T>
+__device__ __forceinline__ void mma16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1);
+
+template <>
+__device__ __forceinline__ void mma16816<__half>(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <>
+__device__ __forceinline__ void mma16816<__nv_bfloat16>(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t& r0, uint32_t& r1, uint32_t addr) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(addr));
+}
+__device__ __forceinline__ uint32_t at_smem(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void at_cp16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kAcThreads, 1)
+altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, const float* __restrict__ coords,
+                        const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, T* __restrict__ corr,
+                        int N1, int N2, int H, int W, int H2, int W2, int M, int r, int32_t* __restrict__ info) {
+  constexpr int C = 128;
+  extern __shared__ __align__(16) uint8_t at_raw[];
+  T* As = reinterpret_cast<T*>(at_raw);                                         // [64][kAtLd]
+  T* Bs = As + kAtPix * kAtLd;                                                  // [kAtMaxPos][kAtLd]
+  float* Ds = reinterpret_cast<float*>(Bs + kAtMaxPos * kAtLd);                 // [64][kAtDLd]
+  float4* geo = reinterpret_cast<float4*>(Ds + kAtPix * kAtDLd);               // [64]
+  int* box = reinterpret_cast<int*>(geo + kAtPix);                              // x0 min, y0 min, x0 max, y0 max
+  const int b = blockIdx.z, m = blockIdx.y;
+  const int HW = H * W;
+  const int ntx = (W + kAtSide - 1) / kAtSide;
+  const int tx0 = (blockIdx.x % ntx) * kAtSide, ty0 = (blockIdx.x / ntx) * kAtSide;
+  const int D = 2 * r + 2, rd = 2 * r + 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t ix = ii[m], jx = jj[m];
+  const bool ok = ix >= 0 && ix < N1 && jx >= 0 && jx < N2;
+  if (!ok && tid == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
+  if (tid == 0) {
+    box[0] = box[1] = 0x7fffffff;
+    box[2] = box[3] = -0x7fffffff;
+  }
+  __syncthreads();
+  const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
+  const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
+  if (tid < kAtPix) {
+    const int px = tx0 + (tid & 7), py = ty0 + (tid >> 3);
+    if (px < W && py < H) {
+      const float x = cx[py * W + px], y = cy[py * W + px];
+      const float fx = floorf(x), fy = floorf(y);
+      const int x0 = (int)fx - r, y0 = (int)fy - r;
+      geo[tid] = make_float4(x - fx, y - fy, __int_as_float(x0), __int_as_float(y0));
+      atomicMin(&box[0], x0);
+      atomicMin(&box[1], y0);
+      atomicMax(&box[2], x0);
+      atomicMax(&box[3], y0);
+    }
+  }
+  __syncthreads();
+  // window positions inside the target image only; an empty box means all taps are 0
+  const int bx0 = max(box[0], 0), by0 = max(box[1], 0);
+  const int bx1 = min(box[2] + D, W2), by1 = min(box[3] + D, H2);
+  const int bw = bx1 - bx0, bh = by1 - by0;
+  const bool empty = !ok || bw <= 0 || bh <= 0;
+  const int npos = empty ? 0 : bw * bh;
+  const bool tiled = npos <= kAtMaxPos;
+  const T* f1 = p1 + ((int64_t)b * N1 + (ok ? ix : 0)) * HW * C;
+  const T* f2 = p2 + ((int64_t)b * N2 + (ok ? jx : 0)) * (int64_t)H2 * W2 * C;
+  if (!empty && tiled) {
+    const int npad = (npos + 7) & ~7;
+    const uint32_t sA = at_smem(As), sB = at_smem(Bs);
+    for (int idx = tid; idx < (kAtPix + npad) * 16; idx += kAcThreads) {
+      const int row = idx >> 4, ch = (idx & 15) * 8;
+      if (row < kAtPix) {
+        const int px = tx0 + (row & 7), py = ty0 + (row >> 3);
+        const bool live = px < W && py < H;
+        at_cp16(sA + (uint32_t)(row * kAtLd + ch) * 2u, live ? (const void*)(f1 + (int64_t)(py * W + px) * C + ch)
+                                                              : (const void*)f1, live ? 16u : 0u);
+      } else {
+        const int n = row - kAtPix;
+        const bool live = n < npos;
+        const int yy = by0 + (live ? n / bw : 0), xx = bx0 + (live ? n % bw : 0);
+        at_cp16(sB + (uint32_t)(n * kAtLd + ch) * 2u,
+                live ? (const void*)(f2 + ((int64_t)yy * W2 + xx) * C + ch) : (const void*)f2, live ? 16u : 0u);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    // warp: m-tile (warp & 3) of 16 pixels, n-tiles of parity (warp >> 2)
+    const int mt = warp & 3;
+    uint32_t af[8][4];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int rr = (lane & 7) + 8 * ((lane >> 3) & 1), kc = 16 * k + 8 * (lane >> 4);
+      ldsm_x4(af[k], sA + (uint32_t)((16 * mt + rr) * kAtLd + kc) * 2u);
+    }
+    const int ntile = npad >> 3;
+    for (int nt = warp >> 2; nt < ntile; nt += 2) {
+      float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        uint32_t b0, b1;
+        const int nr = 8 * nt + (lane & 7), kc = 16 * k + 8 * ((lane >> 3) & 1);
+        ldsm_x2(b0, b1, sB + (uint32_t)(nr * kAtLd + kc) * 2u);
+        mma16816<T>(d, af[k], b0, b1);
+      }
+      const int row = 16 * mt + (lane >> 2), col = 8 * nt + 2 * (lane & 3);
+      *reinterpret_cast<float2*>(&Ds[row * kAtDLd + col]) = make_float2(d[0], d[1]);
+      *reinterpret_cast<float2*>(&Ds[(row + 8) * kAtDLd + col]) = make_float2(d[2], d[3]);
+    }
+  } else if (!empty) {
+    // scattered coordinates: per pixel, one warp computes the D x D window (lanes: 8 positions
+    // x 4 channel groups of 32), stored window-major in the pixel's row of Ds
+    const int pq = lane & 7, g = lane >> 3;
+    for (int q = warp; q < kAtPix; q += kAcThreads / 32) {
+      const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
+      if (px >= W || py >= H) continue;
+      const float4 gq = geo[q];
+      const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
+      const uint4* a = reinterpret_cast<const uint4*>(f1 + (int64_t)(py * W + px) * C) + g * 4;
+      uint4 av[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) av[k] = __ldg(a + k);
+      for (int wy = 0; wy < D; ++wy) {
+        const int y1 = yb + wy;
+        for (int pc = 0; pc < D; pc += 8) {
+          const int wx = pc + pq, x1 = xb + wx;
+          float s0 = 0.f, s1 = 0.f;
+          if (wx < D && y1 >= 0 && y1 < H2 && x1 >= 0 && x1 < W2) {
+            const uint4* bp = reinterpret_cast<const uint4*>(f2 + ((int64_t)y1 * W2 + x1) * C) + g * 4;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) dot8<T>(av[k], __ldg(bp + k), s0, s1);
+          }
+          float sv = s0 + s1;
+          sv += __shfl_xor_sync(0xffffffffu, sv, 8);
+          sv += __shfl_xor_sync(0xffffffffu, sv, 16);
+          if (g == 0 && wx < D) Ds[q * kAtDLd + wy * D + wx] = sv;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // bilinear blend of each output tap from its four window values (0 outside the target)
+  const int nout = rd * rd;
+  T* out = corr + ((int64_t)b * M + m) * nout * HW;
+  for (int idx = tid; idx < kAtPix * nout; idx += kAcThreads) {
+    const int o = idx >> 6, q = idx & 63;
+    const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
+    if (px >= W || py >= H) continue;
+    float v = 0.f;
+    if (!empty) {
+      const int a = o / rd, bb = o - (o / rd) * rd;   // x offset (dim 2), y offset (dim 3)
+      const float4 gq = geo[q];
+      const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
+      const float* dq = Ds + q * kAtDLd;
+      float t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int wx = a + (u & 1), wy = bb + (u >> 1);
+        const int x1 = xb + wx, y1 = yb + wy;
+        t[u] = 0.f;
+        if (x1 >= 0 && x1 < W2 && y1 >= 0 && y1 < H2)
+          t[u] = tiled ? dq[(y1 - by0) * bw + (x1 - bx0)] : dq[wy * D + wx];
+      }
+      v = ((1.f - gq.x) * (1.f - gq.y) * t[0] + gq.x * (1.f - gq.y) * t[1] + (1.f - gq.x) * gq.y * t[2] +
+           gq.x * gq.y * t[3]) * 0.0625f;
+    }
+    out[(int64_t)o * HW + py * W + px] = from_f<T>(v);
+  }
+}
+
 template <typename T>
 __global__ void cast_from_f32_kernel(const float* __restrict__ src, T* __restrict__ dst, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -455,7 +666,28 @@ static int ac_fwd_packed(const void* p1, const void* p2, int b, int n1, int n2, 
   switch (c) {
     case 32: return ac_fwd_packed_n<T, 1>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
     case 64: return ac_fwd_packed_n<T, 2>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
-    case 128: return ac_fwd_packed_n<T, 4>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    case 128: {
+      if (radius <= 8) {   // windows up to 18 x 18 taps
+        static DeviceOnce once;
+        int dev = 0;
+        HS2_CUDA(cudaGetDevice(&dev));
+        int rc = once.run(dev, [&]() -> int {
+          HS2_CUDA(cudaFuncSetAttribute(altcorr_fwd_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kAtSmem));
+          return HS2_OK;
+        });
+        if (rc) return rc;
+        const int ntiles = ((w + kAtSide - 1) / kAtSide) * ((h + kAtSide - 1) / kAtSide);
+        dim3 grid(ntiles, m, b);
+        HS2_PROF("altcorr_fwd_tile", s);
+        altcorr_fwd_tile_kernel<T><<<grid, kAcThreads, kAtSmem, s>>>(
+            static_cast<const T*>(p1), static_cast<const T*>(p2), coords, ii, jj, static_cast<T*>(corr), n1, n2, h,
+            w, h2, w2, m, radius, info);
+        HS2_LAUNCH_CHECK("altcorr_fwd_tile_kernel");
+        return HS2_OK;
+      }
+      return ac_fwd_packed_n<T, 4>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
+    }
     case 256: return ac_fwd_packed_n<T, 8>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
   }
   set_error("altcorr_forward_packed: channels must be 32, 64, 128 or 256 (got %d)", c);

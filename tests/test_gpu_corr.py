@@ -222,3 +222,32 @@ def test_altcorr_packed_frontend_size(cuda):
         slow = blk(coords, c["ii"], c["jj"])
     assert fast.shape == slow.shape == (1, 24, 4 * 49, 43, 77)
     assert rel(np64(fast), np64(slow)) < 2 ** -10
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16], ids=["f16", "bf16"])
+@pytest.mark.parametrize("level,r", [(0, 3), (1, 3), (0, 4), (2, 2)])
+def test_altcorr_tiled_smooth_coords_vs_oracle(cuda, dtype, level, r):
+    """Smooth coordinates (a scaled, shifted pixel grid plus 0.7 px of noise): 8x8 pixel
+    blocks whose windows fit the staged box take the tensor-core path, including blocks
+    whose windows cross the target's borders."""
+    B, N, C, H, W = 1, 3, 128, 20, 30
+    g = torch.Generator().manual_seed(40 + level + r)
+    H2, W2 = H >> level, W >> level
+    f1 = (torch.randn(B, N, C, H, W, generator=g) / np.sqrt(C)).to(cuda, dtype)
+    f2 = (torch.randn(B, N, C, H2, W2, generator=g) / np.sqrt(C)).to(cuda, dtype)
+    ii = torch.tensor([0, 1, 2, 1], device=cuda)
+    jj = torch.tensor([1, 2, 0, 1], device=cuda)
+    v, u = torch.meshgrid(torch.arange(H, dtype=torch.float32), torch.arange(W, dtype=torch.float32), indexing="ij")
+    crd = []
+    for e in range(4):
+        sx, sy = 1.0 / 2 ** level, 1.0 / 2 ** level
+        x = (u * sx + (e - 1.5) * 1.7) + 0.7 * torch.randn(H, W, generator=g)
+        y = (v * sy - (e - 1.5) * 1.1) + 0.7 * torch.randn(H, W, generator=g)
+        crd.append(torch.stack([x, y], 0))
+    crd = torch.stack(crd, 0)[None].contiguous().to(cuda)
+    out, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, r)
+    ref = oc.altcorr_forward(np64(f1), np64(f2), np64(crd), ii.cpu().numpy(), jj.cpu().numpy(), r)
+    tol = 2 ** -10 if dtype == torch.float16 else 2 ** -7
+    assert rel(np64(out), ref) < tol
+    direct, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, r, path="direct")
+    assert rel(np64(out), np64(direct)) < tol
