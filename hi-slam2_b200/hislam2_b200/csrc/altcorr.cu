@@ -354,11 +354,12 @@ altcorr_fwd_packed_kernel(const T* __restrict__ p1, const T* __restrict__ p2, co
 // staging and the gather epilogue, not by the tensor pipe.
 constexpr int kAtSide = 8;
 constexpr int kAtPix = kAtSide * kAtSide;
+constexpr int kAtThreads = 512;        // 16 warps: 4 m-tiles x 4 n-tile phases
 constexpr int kAtMaxPos = 384;
 constexpr int kAtLd = 136;             // halves per staged row: 128 channels + 16 bytes of padding
 constexpr int kAtDLd = kAtMaxPos + 4;  // floats per row of the staged product
 constexpr size_t kAtSmem = (size_t)kAtPix * kAtLd * 2 + (size_t)kAtMaxPos * kAtLd * 2 +
-                           (size_t)kAtPix * kAtDLd * 4 + kAtPix * 16 + 64;
+                           (size_t)kAtPix * kAtDLd * 4 + kAtPix * 16 + 128;
 
 template <typename T>
 __device__ __forceinline__ void mma16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1);
@@ -394,7 +395,7 @@ __device__ __forceinline__ void at_cp16(uint32_t dst, const void* src, uint32_t 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kAcThreads, 1)
+__global__ void __launch_bounds__(kAtThreads, 1)
 altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, const float* __restrict__ coords,
                         const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, T* __restrict__ corr,
                         int N1, int N2, int H, int W, int H2, int W2, int M, int r, int32_t* __restrict__ info) {
@@ -404,7 +405,10 @@ altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, cons
   T* Bs = As + kAtPix * kAtLd;                                                  // [kAtMaxPos][kAtLd]
   float* Ds = reinterpret_cast<float*>(Bs + kAtMaxPos * kAtLd);                 // [64][kAtDLd]
   float4* geo = reinterpret_cast<float4*>(Ds + kAtPix * kAtDLd);               // [64]
-  int* box = reinterpret_cast<int*>(geo + kAtPix);                              // x0 min, y0 min, x0 max, y0 max
+  // box[12]: x0 min, y0 min, x0 max, y0 max of the whole block, then of its top and bottom
+  // halves (rows 0-3, 4-7); reg[8]: per region bx0, by0, bw, mode (0 empty, 1 box, 2 window)
+  int* box = reinterpret_cast<int*>(geo + kAtPix);
+  int* reg = box + 12;
   const int b = blockIdx.z, m = blockIdx.y;
   const int HW = H * W;
   const int ntx = (W + kAtSide - 1) / kAtSide;
@@ -414,10 +418,7 @@ altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, cons
   const int64_t ix = ii[m], jx = jj[m];
   const bool ok = ix >= 0 && ix < N1 && jx >= 0 && jx < N2;
   if (!ok && tid == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
-  if (tid == 0) {
-    box[0] = box[1] = 0x7fffffff;
-    box[2] = box[3] = -0x7fffffff;
-  }
+  if (tid < 12) box[tid] = (tid & 3) < 2 ? 0x7fffffff : -0x7fffffff;
   __syncthreads();
   const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
   const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
@@ -428,122 +429,181 @@ altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, cons
       const float fx = floorf(x), fy = floorf(y);
       const int x0 = (int)fx - r, y0 = (int)fy - r;
       geo[tid] = make_float4(x - fx, y - fy, __int_as_float(x0), __int_as_float(y0));
+      int* bh = box + 4 * (1 + (tid >> 5));
       atomicMin(&box[0], x0);
       atomicMin(&box[1], y0);
       atomicMax(&box[2], x0);
       atomicMax(&box[3], y0);
+      atomicMin(&bh[0], x0);
+      atomicMin(&bh[1], y0);
+      atomicMax(&bh[2], x0);
+      atomicMax(&bh[3], y0);
     }
   }
   __syncthreads();
-  // window positions inside the target image only; an empty box means all taps are 0
-  const int bx0 = max(box[0], 0), by0 = max(box[1], 0);
-  const int bx1 = min(box[2] + D, W2), by1 = min(box[3] + D, H2);
-  const int bw = bx1 - bx0, bh = by1 - by0;
-  const bool empty = !ok || bw <= 0 || bh <= 0;
-  const int npos = empty ? 0 : bw * bh;
-  const bool tiled = npos <= kAtMaxPos;
+  // regions: the whole block when its box (window positions inside the target only) fits
+  // the staging area, else its two halves, each staged if it fits and computed per pixel
+  // otherwise; an empty box means all of the region's taps are 0
+  auto box_of = [&](const int* bb, int& x0, int& y0, int& w, int& h) {
+    if (bb[0] > bb[2]) {   // no pixel in the region
+      x0 = y0 = w = h = 0;
+      return;
+    }
+    x0 = max(bb[0], 0);
+    y0 = max(bb[1], 0);
+    w = min(min(bb[2], W2) + D, W2) - x0;
+    h = min(min(bb[3], H2) + D, H2) - y0;
+    if (w <= 0 || h <= 0) w = h = 0;
+  };
+  int fx0, fy0, fw, fh;
+  box_of(box, fx0, fy0, fw, fh);
+  const int nreg = (ok && fw * fh > kAtMaxPos) ? 2 : 1;
   const T* f1 = p1 + ((int64_t)b * N1 + (ok ? ix : 0)) * HW * C;
   const T* f2 = p2 + ((int64_t)b * N2 + (ok ? jx : 0)) * (int64_t)H2 * W2 * C;
-  if (!empty && tiled) {
-    const int npad = (npos + 7) & ~7;
-    const uint32_t sA = at_smem(As), sB = at_smem(Bs);
-    for (int idx = tid; idx < (kAtPix + npad) * 16; idx += kAcThreads) {
-      const int row = idx >> 4, ch = (idx & 15) * 8;
-      if (row < kAtPix) {
-        const int px = tx0 + (row & 7), py = ty0 + (row >> 3);
-        const bool live = px < W && py < H;
-        at_cp16(sA + (uint32_t)(row * kAtLd + ch) * 2u, live ? (const void*)(f1 + (int64_t)(py * W + px) * C + ch)
-                                                              : (const void*)f1, live ? 16u : 0u);
-      } else {
-        const int n = row - kAtPix;
-        const bool live = n < npos;
-        const int yy = by0 + (live ? n / bw : 0), xx = bx0 + (live ? n % bw : 0);
-        at_cp16(sB + (uint32_t)(n * kAtLd + ch) * 2u,
-                live ? (const void*)(f2 + ((int64_t)yy * W2 + xx) * C + ch) : (const void*)f2, live ? 16u : 0u);
-      }
+  const uint32_t sA = at_smem(As), sB = at_smem(Bs);
+  bool a_staged = false;
+  for (int rg = 0; rg < nreg; ++rg) {
+    int bx0, by0, bw, bh;
+    if (nreg == 1) {
+      bx0 = fx0, by0 = fy0, bw = fw, bh = fh;
+    } else {
+      box_of(box + 4 * (1 + rg), bx0, by0, bw, bh);
     }
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-    __syncthreads();
-    // warp: m-tile (warp & 3) of 16 pixels, n-tiles of parity (warp >> 2)
-    const int mt = warp & 3;
-    uint32_t af[8][4];
+    const int npos = ok ? bw * bh : 0;
+    const int mode = npos == 0 ? 0 : (npos <= kAtMaxPos ? 1 : 2);
+    const int r0 = nreg == 1 ? 0 : 32 * rg, nrows = nreg == 1 ? kAtPix : 32;
+    if (tid == 0) {
+      reg[4 * rg + 0] = bx0;
+      reg[4 * rg + 1] = by0;
+      reg[4 * rg + 2] = bw;
+      reg[4 * rg + 3] = mode;
+    }
+    if (mode == 1) {
+      const int npad = (npos + 7) & ~7;
+      const int arows = a_staged ? 0 : kAtPix;
+      // n / bw without an integer division: for the staged box (n, bw <= 384) (n + 0.5) / bw
+      // stays at least 0.5 / bw from an integer, far beyond the float rounding
+      const float inv_bw = 1.f / (float)bw;
+      // one item = a quarter row (four 16-byte copies): the row's address is formed once
+      for (int idx = tid; idx < (arows + npad) * 4; idx += kAtThreads) {
+        const int row = idx >> 2, ch0 = (idx & 3) * 32;
+        const T* src;
+        uint32_t dst, bytes;
+        if (row < arows) {
+          const int px = tx0 + (row & 7), py = ty0 + (row >> 3);
+          const bool live = px < W && py < H;
+          src = live ? f1 + (int64_t)(py * W + px) * C + ch0 : f1;
+          bytes = live ? 16u : 0u;
+          dst = sA + (uint32_t)(row * kAtLd + ch0) * 2u;
+        } else {
+          const int n = row - arows;
+          const bool live = n < npos;
+          const int qy = __float2int_rz(((float)n + 0.5f) * inv_bw);
+          src = live ? f2 + ((int64_t)(by0 + qy) * W2 + bx0 + n - qy * bw) * C + ch0 : f2;
+          bytes = live ? 16u : 0u;
+          dst = sB + (uint32_t)(n * kAtLd + ch0) * 2u;
+        }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int rr = (lane & 7) + 8 * ((lane >> 3) & 1), kc = 16 * k + 8 * (lane >> 4);
-      ldsm_x4(af[k], sA + (uint32_t)((16 * mt + rr) * kAtLd + kc) * 2u);
-    }
-    const int ntile = npad >> 3;
-    for (int nt = warp >> 2; nt < ntile; nt += 2) {
-      float d[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int u = 0; u < 4; ++u) at_cp16(dst + 16u * u, bytes ? (const void*)(src + 8 * u) : (const void*)src, bytes);
+      }
+      a_staged = true;
+      asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+      // warp: one of the region's m-tiles (16 pixels), n-tiles strided over the other warps
+      const int nmt = nrows >> 4;
+      const int mt = (r0 >> 4) + warp % nmt;
+      const int nstep = (kAtThreads / 32) / nmt;   // 4 (whole block) or 8 (half) n-tile phases
+      uint32_t af[8][4];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        uint32_t b0, b1;
-        const int nr = 8 * nt + (lane & 7), kc = 16 * k + 8 * ((lane >> 3) & 1);
-        ldsm_x2(b0, b1, sB + (uint32_t)(nr * kAtLd + kc) * 2u);
-        mma16816<T>(d, af[k], b0, b1);
+        const int rr = (lane & 7) + 8 * ((lane >> 3) & 1), kc = 16 * k + 8 * (lane >> 4);
+        ldsm_x4(af[k], sA + (uint32_t)((16 * mt + rr) * kAtLd + kc) * 2u);
       }
-      const int row = 16 * mt + (lane >> 2), col = 8 * nt + 2 * (lane & 3);
-      *reinterpret_cast<float2*>(&Ds[row * kAtDLd + col]) = make_float2(d[0], d[1]);
-      *reinterpret_cast<float2*>(&Ds[(row + 8) * kAtDLd + col]) = make_float2(d[2], d[3]);
-    }
-  } else if (!empty) {
-    // scattered coordinates: per pixel, one warp computes the D x D window (lanes: 8 positions
-    // x 4 channel groups of 32), stored window-major in the pixel's row of Ds
-    const int pq = lane & 7, g = lane >> 3;
-    for (int q = warp; q < kAtPix; q += kAcThreads / 32) {
-      const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
-      if (px >= W || py >= H) continue;
-      const float4 gq = geo[q];
-      const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
-      const uint4* a = reinterpret_cast<const uint4*>(f1 + (int64_t)(py * W + px) * C) + g * 4;
-      uint4 av[4];
+      const int ntile = npad >> 3;
+      for (int nt = warp / nmt; nt < ntile; nt += nstep) {
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-      for (int k = 0; k < 4; ++k) av[k] = __ldg(a + k);
-      for (int wy = 0; wy < D; ++wy) {
-        const int y1 = yb + wy;
-        for (int pc = 0; pc < D; pc += 8) {
-          const int wx = pc + pq, x1 = xb + wx;
-          float s0 = 0.f, s1 = 0.f;
-          if (wx < D && y1 >= 0 && y1 < H2 && x1 >= 0 && x1 < W2) {
-            const uint4* bp = reinterpret_cast<const uint4*>(f2 + ((int64_t)y1 * W2 + x1) * C) + g * 4;
+        for (int k = 0; k < 8; ++k) {
+          uint32_t b0, b1;
+          const int nr = 8 * nt + (lane & 7), kc = 16 * k + 8 * ((lane >> 3) & 1);
+          ldsm_x2(b0, b1, sB + (uint32_t)(nr * kAtLd + kc) * 2u);
+          mma16816<T>(d, af[k], b0, b1);
+        }
+        const int row = 16 * mt + (lane >> 2), col = 8 * nt + 2 * (lane & 3);
+        *reinterpret_cast<float2*>(&Ds[row * kAtDLd + col]) = make_float2(d[0], d[1]);
+        *reinterpret_cast<float2*>(&Ds[(row + 8) * kAtDLd + col]) = make_float2(d[2], d[3]);
+      }
+      __syncthreads();   // the staging area is reused by the next region
+    } else if (mode == 2) {
+      // scattered coordinates: per pixel, one warp computes the D x D window (lanes: 8
+      // positions x 4 channel groups of 32), stored window-major in the pixel's row of Ds
+      const int pq = lane & 7, g = lane >> 3;
+      for (int q = r0 + warp; q < r0 + nrows; q += kAtThreads / 32) {
+        const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
+        if (px >= W || py >= H) continue;
+        const float4 gq = geo[q];
+        const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
+        const uint4* a = reinterpret_cast<const uint4*>(f1 + (int64_t)(py * W + px) * C) + g * 4;
+        uint4 av[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) dot8<T>(av[k], __ldg(bp + k), s0, s1);
+        for (int k = 0; k < 4; ++k) av[k] = __ldg(a + k);
+        for (int wy = 0; wy < D; ++wy) {
+          const int y1 = yb + wy;
+          for (int pc = 0; pc < D; pc += 8) {
+            const int wx = pc + pq, x1 = xb + wx;
+            float s0 = 0.f, s1 = 0.f;
+            if (wx < D && y1 >= 0 && y1 < H2 && x1 >= 0 && x1 < W2) {
+              const uint4* bp = reinterpret_cast<const uint4*>(f2 + ((int64_t)y1 * W2 + x1) * C) + g * 4;
+#pragma unroll
+              for (int k = 0; k < 4; ++k) dot8<T>(av[k], __ldg(bp + k), s0, s1);
+            }
+            float sv = s0 + s1;
+            sv += __shfl_xor_sync(0xffffffffu, sv, 8);
+            sv += __shfl_xor_sync(0xffffffffu, sv, 16);
+            if (g == 0 && wx < D) Ds[q * kAtDLd + wy * D + wx] = sv;
           }
-          float sv = s0 + s1;
-          sv += __shfl_xor_sync(0xffffffffu, sv, 8);
-          sv += __shfl_xor_sync(0xffffffffu, sv, 16);
-          if (g == 0 && wx < D) Ds[q * kAtDLd + wy * D + wx] = sv;
         }
       }
     }
   }
   __syncthreads();
-  // bilinear blend of each output tap from its four window values (0 outside the target)
+  // bilinear blend: thread (pixel q, x offset a) walks the window rows, keeping the two
+  // values of the previous row, so each output reads two new window values; taps outside
+  // the target are 0
   const int nout = rd * rd;
   T* out = corr + ((int64_t)b * M + m) * nout * HW;
-  for (int idx = tid; idx < kAtPix * nout; idx += kAcThreads) {
-    const int o = idx >> 6, q = idx & 63;
+  for (int idx = tid; idx < kAtPix * rd; idx += kAtThreads) {
+    const int q = idx & 63, a = idx >> 6;
     const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
     if (px >= W || py >= H) continue;
-    float v = 0.f;
-    if (!empty) {
-      const int a = o / rd, bb = o - (o / rd) * rd;   // x offset (dim 2), y offset (dim 3)
-      const float4 gq = geo[q];
-      const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
-      const float* dq = Ds + q * kAtDLd;
-      float t[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int wx = a + (u & 1), wy = bb + (u >> 1);
-        const int x1 = xb + wx, y1 = yb + wy;
-        t[u] = 0.f;
-        if (x1 >= 0 && x1 < W2 && y1 >= 0 && y1 < H2)
-          t[u] = tiled ? dq[(y1 - by0) * bw + (x1 - bx0)] : dq[wy * D + wx];
-      }
-      v = ((1.f - gq.x) * (1.f - gq.y) * t[0] + gq.x * (1.f - gq.y) * t[1] + (1.f - gq.x) * gq.y * t[2] +
-           gq.x * gq.y * t[3]) * 0.0625f;
+    const int* rq = reg + 4 * (nreg == 1 ? 0 : q >> 5);
+    const int mode = rq[3];
+    T* oq = out + (int64_t)(a * rd) * HW + py * W + px;
+    if (mode == 0) {
+      for (int bb = 0; bb < rd; ++bb) oq[(int64_t)bb * HW] = from_f<T>(0.f);
+      continue;
     }
-    out[(int64_t)o * HW + py * W + px] = from_f<T>(v);
+    const float4 gq = geo[q];
+    const int xb = __float_as_int(gq.z), yb = __float_as_int(gq.w);
+    const int x1 = xb + a;
+    const bool va = x1 >= 0 && x1 < W2, vb = x1 + 1 >= 0 && x1 + 1 < W2;
+    // row-major addressing of the window values: the staged box (mode 1) or the pixel's own
+    // D x D window (mode 2)
+    const int rs = mode == 1 ? rq[2] : D;
+    const float* dq = Ds + q * kAtDLd + (mode == 1 ? (yb - rq[1]) * rs + (x1 - rq[0]) : a);
+    const float w00 = (1.f - gq.x) * (1.f - gq.y), w01 = gq.x * (1.f - gq.y);
+    const float w10 = (1.f - gq.x) * gq.y, w11 = gq.x * gq.y;
+    float t0 = 0.f, t1 = 0.f;
+    for (int wy = 0; wy <= rd; ++wy) {
+      const int y1 = yb + wy;
+      const bool vy = y1 >= 0 && y1 < H2;
+      const float* row = dq + wy * rs;
+      const float u0 = (vy && va) ? row[0] : 0.f, u1 = (vy && vb) ? row[1] : 0.f;
+      if (wy > 0)
+        oq[(int64_t)(wy - 1) * HW] = from_f<T>((w00 * t0 + w01 * t1 + w10 * u0 + w11 * u1) * 0.0625f);
+      t0 = u0;
+      t1 = u1;
+    }
   }
 }
 
@@ -680,7 +740,7 @@ static int ac_fwd_packed(const void* p1, const void* p2, int b, int n1, int n2, 
         const int ntiles = ((w + kAtSide - 1) / kAtSide) * ((h + kAtSide - 1) / kAtSide);
         dim3 grid(ntiles, m, b);
         HS2_PROF("altcorr_fwd_tile", s);
-        altcorr_fwd_tile_kernel<T><<<grid, kAcThreads, kAtSmem, s>>>(
+        altcorr_fwd_tile_kernel<T><<<grid, kAtThreads, kAtSmem, s>>>(
             static_cast<const T*>(p1), static_cast<const T*>(p2), coords, ii, jj, static_cast<T*>(corr), n1, n2, h,
             w, h2, w2, m, radius, info);
         HS2_LAUNCH_CHECK("altcorr_fwd_tile_kernel");
