@@ -496,45 +496,58 @@ def batch_leg(args, dev, world, rank):
 
 
 def altcorr_leg(args, dev, world, peaks):
-    """The backend's memory-light correlation (AltCorrBlock, radius 3, 4 levels) over all
-    6000 edges of the 300-keyframe window, called in the global BA loop's chunks: the edges
-    whose source frame lies in [i, i + 2) (HI-SLAM2 factor_graph.py:253-260).  One step =
-    one pass over every chunk and level (fp16 features, float32 coordinates)."""
-    from hislam2_b200 import backends, synth
-    from hislam2_b200.corr import _pool_pyramid
-    p = synth.make_ba_problem(WORKLOAD, seed=0)
-    g = torch.Generator().manual_seed(17)
-    K, H, W, C, r, L = 300, 43, 77, 128, 3, 4
-    fmaps = (torch.randn(K, C, H, W, generator=g) / np.sqrt(C)).half().to(dev)
-    pyr = [lv[None].contiguous() for lv in _pool_pyramid(fmaps, L)]
-    ii, jj = p["ii"].to(dev), p["jj"].to(dev)
-    coords = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], p["ii"], p["jj"]).float()
-    coords = (coords + torch.randn(coords.shape, generator=g)).permute(0, 3, 1, 2).contiguous().to(dev)
-    chunks = []
-    for i in range(0, int(p["jj"].max()) + 1, 2):
-        v = ((ii >= i) & (ii < i + 2)).nonzero().flatten()
-        if v.numel():
-            chunks.append((ii[v].contiguous(), jj[v].contiguous(),
-                           [(coords[v] / 2 ** lvl)[None].contiguous() for lvl in range(L)]))
+    """The backend's memory-light correlation (radius 3, 4 levels, float16 features) over all
+    6000 edges of the 300-keyframe window in the global BA loop's chunks of two source
+    frames (HI-SLAM2 factor_graph.py:253-260); one step = one pass over every chunk and
+    level.  `dropin`: droid_backends.altcorr_forward per chunk and level (it packs the
+    call's frames channel-last first); `block`: AltCorrBlock with its pyramid packed once.
+    Algorithmic work per edge-pixel-level: D^2 = 64 window dot products of 128 channels."""
+    from hislam2_b200 import backends
+    from hislam2_b200.corr import AltCorrBlock
+    fmaps, pyr, chunks = altcorr_inputs(dev)
+    r, L, E, H, W, C = 3, 4, 6000, 43, 77, 128
 
-    def step():
+    def dropin():
         for ci, cj, crd in chunks:
             for lvl in range(L):
                 backends.altcorr_forward(pyr[0], pyr[lvl], crd[lvl], ci, cj, r)
 
+    blk = AltCorrBlock(fmaps[None].contiguous(), num_levels=L, radius=r)
+    crd5 = [(ci, cj, crd[0].permute(0, 1, 3, 4, 2).contiguous()) for ci, cj, crd in chunks]
+
+    def block():
+        with torch.no_grad():
+            for ci, cj, crd in crd5:
+                blk(crd, ci, cj)
+
+    from hislam2_b200 import synth
+    pb = synth.make_ba_problem(WORKLOAD, seed=0, device=dev)
+    levels = [lv[0] for lv in pyr]
+
+    def fused():
+        for ci, cj, _ in chunks:
+            backends.corr_reproject_lookup(levels, pb["poses"], pb["disps"], pb["intrinsics"], ci, cj, r)
+
     steps = max(3, min(args.steps, 10))
     barrier(world)
-    ms = max_over_ranks(device_time(step, steps), world, dev)
-    E = ii.numel()
-    taps = (2 * r + 1) ** 2
-    flops = sum(2.0 * E * H * W * taps * C for _ in range(L))
-    out_bytes = E * H * W * taps * L * 2
+    ms_drop = max_over_ranks(device_time(dropin, steps), world, dev)
+    ms_blk = max_over_ranks(device_time(block, steps), world, dev)
+    ms_fused = max_over_ranks(device_time(fused, steps), world, dev)
+    D = 2 * r + 2
+    flops = 2.0 * E * H * W * D * D * C * L
+    out_bytes = E * H * W * (2 * r + 1) ** 2 * L * 2
     res = {"config": "300 keyframes, 6000 edges, 43x77, 128 channels fp16, radius 3, 4 levels, %d chunks of "
                      "two source frames" % len(chunks),
-           "ms_per_pass": round(ms, 3), "edges_per_s": round(E / (ms / 1e3) * world, 1),
-           "tflops_fp32_simt": round(flops / (ms / 1e3) / 1e12, 2), "write_gbs": round(out_bytes / (ms / 1e3) / 1e9, 1),
+           "dropin": {"ms_per_pass": round(ms_drop, 3), "edges_per_s": round(E / (ms_drop / 1e3) * world, 1)},
+           "block": {"ms_per_pass": round(ms_blk, 3), "edges_per_s": round(E / (ms_blk / 1e3) * world, 1),
+                     "tflops": round(flops / (ms_blk / 1e3) / 1e12, 2),
+                     "write_gbs": round(out_bytes / (ms_blk / 1e3) / 1e9, 1)},
+           "fused_reproject_lookup": {
+               "ms_per_pass": round(ms_fused, 3), "edges_per_s": round(E / (ms_fused / 1e3) * world, 1),
+               "note": "corr_reproject_lookup per chunk: coordinates reprojected from the current poses and "
+                       "disparities inside the kernel (no coordinate or volume tensors), same chunks"},
            "algorithmic": {"gflop": round(flops / 1e9, 1), "write_gb": round(out_bytes / 1e9, 3)}}
-    del pyr, chunks
+    del pyr, chunks, blk, crd5, levels
     torch.cuda.empty_cache()
     return res
 
@@ -795,6 +808,7 @@ def run_reference(args, world, rank):
     total = float(sum(times))
     value = args.steps * iters / total
     corr = reference_corr_lookup(ref, args, dev)
+    alt = reference_altcorr(ref, dev)
     line = dict(common, value=round(value, 4), warmup=args.warmup, ms_per_step=round(1e3 * total / args.steps, 3),
                 dtype="f32 kernels, f64 host solve",
                 config=dict(CONFIG, parallelism="single GPU + host", iterations_per_step=iters),
@@ -805,8 +819,58 @@ def run_reference(args, world, rank):
                                         "window, %d GN iteration(s) per step: CUDA kernels on the GPU, host loops, "
                                         "triplet assembly and the solve on one host core" % iters},
                 e2e={"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                corr_lookup=corr)
+                corr_lookup=corr, altcorr=alt)
     print(json.dumps(line), flush=True)
+
+
+def altcorr_inputs(dev, dtype=torch.float16):
+    """The backend's correlation workload: 300 keyframes of 128-channel features at 43x77
+    (~N(0,1)/sqrt(128)), the 4-level pooled pyramid, and the 6000 edges' reprojected
+    coordinates (+ N(0,1) px) in the global BA loop's chunks of two source frames
+    (factor_graph.py:253-260), coordinates pre-scaled per level, [1, m, 2, H, W]."""
+    from hislam2_b200 import synth
+    from hislam2_b200.corr import _pool_pyramid
+    p = synth.make_ba_problem(WORKLOAD, seed=0)
+    g = torch.Generator().manual_seed(17)
+    K, H, W, C, L = 300, 43, 77, 128, 4
+    fmaps = (torch.randn(K, C, H, W, generator=g) / np.sqrt(C)).to(dev, dtype)
+    pyr = [lv[None].contiguous() for lv in _pool_pyramid(fmaps, L)]
+    ii, jj = p["ii"].to(dev), p["jj"].to(dev)
+    coords = synth.reproject(p["poses_gt"], p["disps_gt"], p["intrinsics"], p["ii"], p["jj"]).float()
+    coords = (coords + torch.randn(coords.shape, generator=g)).permute(0, 3, 1, 2).contiguous().to(dev)
+    chunks = []
+    for i in range(0, int(p["jj"].max()) + 1, 2):
+        v = ((ii >= i) & (ii < i + 2)).nonzero().flatten()
+        if v.numel():
+            chunks.append((ii[v].contiguous(), jj[v].contiguous(),
+                           [(coords[v] / 2 ** lvl)[None].contiguous() for lvl in range(L)]))
+    return fmaps, pyr, chunks
+
+
+def reference_altcorr(ref, dev):
+    """The reference's altcorr_forward (src/altcorr_kernel.cu, built in oracle/_ref) over the
+    same 6000-edge backend pass as the `altcorr` leg (float16 features, radius 3, 4 levels),
+    one pass timed with CUDA events after one warm-up chunk."""
+    _, pyr, chunks = altcorr_inputs(dev)
+
+    def run(chs):
+        for ci, cj, crd in chs:
+            for lvl in range(4):
+                ref.altcorr_forward(pyr[0], pyr[lvl], crd[lvl], ci, cj, 3)
+
+    run(chunks[:1])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run(chunks)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    del pyr, chunks
+    torch.cuda.empty_cache()
+    return {"ms_per_pass": round(ms, 2), "edges_per_s": round(6000 / (ms / 1e3), 1),
+            "config": "300 keyframes, 6000 edges in chunks of two source frames, 43x77, 128 channels fp16, "
+                      "radius 3, 4 levels; one pass"}
 
 
 def reference_corr_lookup(ref, args, dev):

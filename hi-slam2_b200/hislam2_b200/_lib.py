@@ -81,6 +81,8 @@ class BaWindow(ctypes.Structure):
 SIGNATURES.update({
     "hs2_corr_reproject_lookup": [_p, _i64, _p, _i64, _p, _p, _i32, _i32, _i64, _i32, _i32, _i32, _p, _p, _i64,
                                   _i32, _p, _p, _p, _p],
+    "hs2_corr_reproject_lookup_packed": [_p, _i64, _p, _i64, _p, _p, _i32, _i32, _i64, _i32, _i32, _i32, _p, _p,
+                                         _i64, _i32, _p, _p, _p, _p],
     "hs2_ba_batch_workspace_size": [ctypes.POINTER(BaWindow), _i32, ctypes.POINTER(_sz)],
     "hs2_ba_batch_prepare": [ctypes.POINTER(BaWindow), _i32, _i32, _i32, _p, _sz, ctypes.POINTER(_i32), _p],
     "hs2_ba_batch_run": [_p, _i32, _i32, _i32, _f32, _f32, _p],

@@ -643,7 +643,8 @@ def corr_volume(fmap1, fmap2, ii=None, jj=None, num_levels=4, precision="native"
     return pyr
 
 
-def corr_reproject_lookup(fmap_levels, poses, disps, intrinsics, ii, jj, radius, return_coords=True):
+def corr_reproject_lookup(fmap_levels, poses, disps, intrinsics, ii, jj, radius, return_coords=True, *,
+                          path="auto"):
     """Reprojection + multi-level correlation lookup in one launch.
 
     Fuses ``DepthVideo.reproject(ii, jj)`` (``hislam2/depth_video.py:170-178``) with the
@@ -651,7 +652,9 @@ def corr_reproject_lookup(fmap_levels, poses, disps, intrinsics, ii, jj, radius,
     list of pooled features [K, C, H>>l, W>>l] (level 0 the features themselves),
     ``poses`` [K,7], ``disps`` [K,H,W], ``intrinsics`` [4] float32.  Returns ``corr``
     [E, L*(2r+1)^2, H, W] (the fmaps' dtype) and, with ``return_coords``, the level-0
-    ``coords1`` [E, H, W, 2] (float32).
+    ``coords1`` [E, H, W, 2] (float32).  float16 / bfloat16 features with 128 channels and
+    radius <= 8 take the channel-last tensor-core path (the frames of ii / jj packed per
+    level first) unless ``path="direct"``.
     """
     L = len(fmap_levels)
     f0 = fmap_levels[0]
@@ -678,6 +681,20 @@ def corr_reproject_lookup(fmap_levels, poses, disps, intrinsics, ii, jj, radius,
     corr = torch.empty(E, L * (2 * r + 1) ** 2, H, W, dtype=f0.dtype, device=dev)
     coords = torch.empty(E, H, W, 2, dtype=torch.float32, device=dev) if return_coords else None
     info = torch.zeros(1, dtype=torch.int32, device=dev)
+    if path not in ("auto", "direct", "packed"):
+        raise RuntimeError("corr_reproject_lookup: path is auto, direct or packed")
+    packable = f0.dtype in (torch.float16, torch.bfloat16) and C == 128 and r <= 8
+    if path == "packed" and not packable:
+        raise RuntimeError("corr_reproject_lookup: the packed path takes float16 / bfloat16 features, C = 128, r <= 8")
+    if packable and path != "direct":
+        both = torch.cat([ii, jj])
+        packed = [PackedFeatures(f[None], both if lvl == 0 else jj) for lvl, f in enumerate(fmap_levels)]
+        pptrs = (ctypes.c_void_p * 4)(*[pk.buf.data_ptr() for pk in packed] + [0] * (4 - L))
+        _lib.check(_lib.load().hs2_corr_reproject_lookup_packed(
+            _ptr(poses), poses.shape[0], _ptr(disps), disps.shape[0], _ptr(intrinsics), pptrs, L, _DTYPES[f0.dtype],
+            K, C, H, W, _ptr(ii), _ptr(jj), E, r, _ptr(corr), _ptr(coords), _ptr(info), _stream(dev)),
+            "corr_reproject_lookup")
+        return (corr, coords) if return_coords else corr
     ptrs = (ctypes.c_void_p * 4)(*[f.data_ptr() for f in fmap_levels] + [0] * (4 - L))
     _lib.check(_lib.load().hs2_corr_reproject_lookup(_ptr(poses), poses.shape[0], _ptr(disps), disps.shape[0],
                                                      _ptr(intrinsics), ptrs, L, _DTYPES[f0.dtype], K, C, H, W,

@@ -394,12 +394,40 @@ __device__ __forceinline__ void at_cp16(uint32_t dst, const void* src, uint32_t 
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 
-template <typename T>
+// Arguments of the tile kernel.  altcorr: window coordinates read from `coords`
+// [B][M][2][H][W], target features p2[0], output [B][M][2r+1][2r+1][H][W].  Fused
+// reprojection + lookup (kFused): blockIdx.z is the level, coordinates are the
+// reprojection of frame ii's pixels into frame jj (poses, disps, intrinsics; the float
+// formula of corr_fused.cu) scaled by 2^-level, target features p2[level], output
+// [M][levels * (2r+1)^2][H][W], and the level-0 coordinates optionally to coords_out.
+struct AtArgs {
+  const void* p1;
+  const void* p2[4];
+  const float* coords;
+  const int64_t* ii;
+  const int64_t* jj;
+  void* corr;
+  int N1, N2, H, W, H2, W2, M, r, levels;
+  int32_t* info;
+  const float* poses;
+  const float* disps;
+  const float* intr;
+  int64_t num_poses, num_disps;
+  float* coords_out;
+};
+
+template <typename T, bool kFused>
 __global__ void __launch_bounds__(kAtThreads, 1)
-altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, const float* __restrict__ coords,
-                        const int64_t* __restrict__ ii, const int64_t* __restrict__ jj, T* __restrict__ corr,
-                        int N1, int N2, int H, int W, int H2, int W2, int M, int r, int32_t* __restrict__ info) {
+altcorr_fwd_tile_kernel(const __grid_constant__ AtArgs A) {
   constexpr int C = 128;
+  const int H = A.H, W = A.W, r = A.r, M = A.M, N1 = A.N1, N2 = A.N2;
+  const int lvl = kFused ? (int)blockIdx.z : 0;
+  const int H2 = kFused ? H >> lvl : A.H2, W2 = kFused ? W >> lvl : A.W2;
+  const int64_t* __restrict__ ii = A.ii;
+  const int64_t* __restrict__ jj = A.jj;
+  const T* __restrict__ p1 = static_cast<const T*>(A.p1);
+  const T* __restrict__ p2 = static_cast<const T*>(A.p2[kFused ? lvl : 0]);
+  __shared__ float G[12];   // fused: R (row-major) then t of Gij
   extern __shared__ __align__(16) uint8_t at_raw[];
   T* As = reinterpret_cast<T*>(at_raw);                                         // [64][kAtLd]
   T* Bs = As + kAtPix * kAtLd;                                                  // [kAtMaxPos][kAtLd]
@@ -409,23 +437,58 @@ altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, cons
   // halves (rows 0-3, 4-7); reg[8]: per region bx0, by0, bw, mode (0 empty, 1 box, 2 window)
   int* box = reinterpret_cast<int*>(geo + kAtPix);
   int* reg = box + 12;
-  const int b = blockIdx.z, m = blockIdx.y;
+  const int b = kFused ? 0 : (int)blockIdx.z, m = blockIdx.y;
   const int HW = H * W;
   const int ntx = (W + kAtSide - 1) / kAtSide;
   const int tx0 = (blockIdx.x % ntx) * kAtSide, ty0 = (blockIdx.x / ntx) * kAtSide;
   const int D = 2 * r + 2, rd = 2 * r + 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t ix = ii[m], jx = jj[m];
-  const bool ok = ix >= 0 && ix < N1 && jx >= 0 && jx < N2;
-  if (!ok && tid == 0 && blockIdx.x == 0 && info) atomicOr(info, HS2_DEV_BAD_INDEX);
+  const bool ok = kFused ? (ix >= 0 && jx >= 0 && ix < N1 && jx < N1 && ix < A.num_poses && jx < A.num_poses &&
+                            ix < A.num_disps)
+                         : (ix >= 0 && ix < N1 && jx >= 0 && jx < N2);
+  if (!ok && tid == 0 && blockIdx.x == 0 && lvl == 0 && A.info) atomicOr(A.info, HS2_DEV_BAD_INDEX);
   if (tid < 12) box[tid] = (tid & 3) < 2 ? 0x7fffffff : -0x7fffffff;
+  if (kFused && tid == 0) {
+    float t[3], q[4];
+    if (ok) {
+      relative_pose(A.poses + 7 * ix, A.poses + 7 * ix + 3, A.poses + 7 * jx, A.poses + 7 * jx + 3, t, q);
+    } else {
+      t[0] = t[1] = t[2] = 0.f;
+      q[0] = q[1] = q[2] = 0.f;
+      q[3] = 1.f;
+    }
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    G[0] = 1.f - 2.f * (y * y + z * z); G[1] = 2.f * (x * y - z * w);       G[2] = 2.f * (x * z + y * w);
+    G[3] = 2.f * (x * y + z * w);       G[4] = 1.f - 2.f * (x * x + z * z); G[5] = 2.f * (y * z - x * w);
+    G[6] = 2.f * (x * z - y * w);       G[7] = 2.f * (y * z + x * w);       G[8] = 1.f - 2.f * (x * x + y * y);
+    G[9] = t[0]; G[10] = t[1]; G[11] = t[2];
+  }
   __syncthreads();
-  const float* cx = coords + (((int64_t)b * M + m) * 2 + 0) * HW;
-  const float* cy = coords + (((int64_t)b * M + m) * 2 + 1) * HW;
   if (tid < kAtPix) {
     const int px = tx0 + (tid & 7), py = ty0 + (tid >> 3);
     if (px < W && py < H) {
-      const float x = cx[py * W + px], y = cy[py * W + px];
+      float x, y;
+      if (kFused) {
+        const float fx = A.intr[0], fy = A.intr[1], cx = A.intr[2], cy = A.intr[3];
+        const int pix = py * W + px;
+        const float d = ok ? A.disps[ix * HW + pix] : 0.f;
+        const float X = (px - cx) / fx, Y = (py - cy) / fy;
+        const float P0 = G[0] * X + G[1] * Y + G[2] + G[9] * d;
+        const float P1 = G[3] * X + G[4] * Y + G[5] + G[10] * d;
+        const float P2 = G[6] * X + G[7] * Y + G[8] + G[11] * d;
+        const float xc = fx * (P0 / P2) + cx, yc = fy * (P1 / P2) + cy;
+        if (lvl == 0 && A.coords_out) {
+          A.coords_out[((int64_t)m * HW + pix) * 2 + 0] = xc;
+          A.coords_out[((int64_t)m * HW + pix) * 2 + 1] = yc;
+        }
+        const float scale = 1.0f / (float)(1 << lvl);
+        x = xc * scale;
+        y = yc * scale;
+      } else {
+        x = A.coords[(((int64_t)b * M + m) * 2 + 0) * HW + py * W + px];
+        y = A.coords[(((int64_t)b * M + m) * 2 + 1) * HW + py * W + px];
+      }
       const float fx = floorf(x), fy = floorf(y);
       const int x0 = (int)fx - r, y0 = (int)fy - r;
       geo[tid] = make_float4(x - fx, y - fy, __int_as_float(x0), __int_as_float(y0));
@@ -571,7 +634,7 @@ altcorr_fwd_tile_kernel(const T* __restrict__ p1, const T* __restrict__ p2, cons
   // values of the previous row, so each output reads two new window values; taps outside
   // the target are 0
   const int nout = rd * rd;
-  T* out = corr + ((int64_t)b * M + m) * nout * HW;
+  T* out = static_cast<T*>(A.corr) + (kFused ? ((int64_t)m * A.levels + lvl) : ((int64_t)b * M + m)) * nout * HW;
   for (int idx = tid; idx < kAtPix * rd; idx += kAtThreads) {
     const int q = idx & 63, a = idx >> 6;
     const int px = tx0 + (q & 7), py = ty0 + (q >> 3);
@@ -719,6 +782,18 @@ static int ac_fwd_packed_n(const void* p1, const void* p2, int b, int n1, int n2
   return HS2_OK;
 }
 
+template <typename T, bool kFused>
+static int at_prepare() {
+  static DeviceOnce once;
+  int dev = 0;
+  HS2_CUDA(cudaGetDevice(&dev));
+  return once.run(dev, [&]() -> int {
+    HS2_CUDA(cudaFuncSetAttribute(altcorr_fwd_tile_kernel<T, kFused>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kAtSmem));
+    return HS2_OK;
+  });
+}
+
 template <typename T>
 static int ac_fwd_packed(const void* p1, const void* p2, int b, int n1, int n2, int c, int h, int w, int h2, int w2,
                          const float* coords, const int64_t* ii, const int64_t* jj, int m, int radius, void* corr,
@@ -728,21 +803,21 @@ static int ac_fwd_packed(const void* p1, const void* p2, int b, int n1, int n2, 
     case 64: return ac_fwd_packed_n<T, 2>(p1, p2, b, n1, n2, h, w, h2, w2, coords, ii, jj, m, radius, corr, info, s);
     case 128: {
       if (radius <= 8) {   // windows up to 18 x 18 taps
-        static DeviceOnce once;
-        int dev = 0;
-        HS2_CUDA(cudaGetDevice(&dev));
-        int rc = once.run(dev, [&]() -> int {
-          HS2_CUDA(cudaFuncSetAttribute(altcorr_fwd_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kAtSmem));
-          return HS2_OK;
-        });
+        int rc = at_prepare<T, false>();
         if (rc) return rc;
+        AtArgs a{};
+        a.p1 = p1;
+        a.p2[0] = p2;
+        a.coords = coords;
+        a.ii = ii;
+        a.jj = jj;
+        a.corr = corr;
+        a.N1 = n1, a.N2 = n2, a.H = h, a.W = w, a.H2 = h2, a.W2 = w2, a.M = m, a.r = radius, a.levels = 1;
+        a.info = info;
         const int ntiles = ((w + kAtSide - 1) / kAtSide) * ((h + kAtSide - 1) / kAtSide);
         dim3 grid(ntiles, m, b);
         HS2_PROF("altcorr_fwd_tile", s);
-        altcorr_fwd_tile_kernel<T><<<grid, kAtThreads, kAtSmem, s>>>(
-            static_cast<const T*>(p1), static_cast<const T*>(p2), coords, ii, jj, static_cast<T*>(corr), n1, n2, h,
-            w, h2, w2, m, radius, info);
+        altcorr_fwd_tile_kernel<T, false><<<grid, kAtThreads, kAtSmem, s>>>(a);
         HS2_LAUNCH_CHECK("altcorr_fwd_tile_kernel");
         return HS2_OK;
       }
@@ -886,4 +961,66 @@ extern "C" int hs2_altcorr_backward(const void* fmap1, const void* fmap2, int dt
   }
   set_error("altcorr_backward: unsupported dtype %d (f32, f16, bf16)", dtype);
   return HS2_ERR_DTYPE;
+}
+
+extern "C" int hs2_corr_reproject_lookup_packed(const float* poses, int64_t num_poses, const float* disps,
+                                                int64_t num_disps, const float* intrinsics,
+                                                const void* const* packed_levels, int levels, int dtype,
+                                                int64_t num_frames, int channels, int ht, int wd, const int64_t* ii,
+                                                const int64_t* jj, int64_t num_edges, int radius, void* corr,
+                                                float* coords1, int32_t* info, hs2_stream_t stream) {
+  using namespace hs2;
+  if (levels < 1 || levels > 4 || radius < 0 || radius > 8 || channels != 128 || ht <= 0 || wd <= 0 ||
+      num_edges < 0 || num_edges > 65535 || num_frames <= 0 || num_frames > (1 << 30) ||
+      (ht >> (levels - 1)) <= 0 || (wd >> (levels - 1)) <= 0) {
+    set_error("corr_reproject_lookup_packed: bad sizes (levels=%d r=%d C=%d ht=%d wd=%d E=%lld K=%lld); "
+              "128 channels and radius <= 8 required", levels, radius, channels, ht, wd, (long long)num_edges,
+              (long long)num_frames);
+    return HS2_ERR_INVALID;
+  }
+  if (dtype != HS2_F16 && dtype != HS2_BF16) {
+    set_error("corr_reproject_lookup_packed: float16 or bfloat16 features only (dtype %d)", dtype);
+    return HS2_ERR_DTYPE;
+  }
+  if (num_edges == 0) return HS2_OK;
+  if (!poses || !disps || !intrinsics || !packed_levels || !ii || !jj || !corr || !info) {
+    set_error("corr_reproject_lookup_packed: null pointer argument");
+    return HS2_ERR_INVALID;
+  }
+  AtArgs a{};
+  for (int l = 0; l < levels; ++l) {
+    if (!packed_levels[l]) {
+      set_error("corr_reproject_lookup_packed: feature level %d missing", l);
+      return HS2_ERR_INVALID;
+    }
+    a.p2[l] = packed_levels[l];
+  }
+  a.p1 = packed_levels[0];
+  a.ii = ii;
+  a.jj = jj;
+  a.corr = corr;
+  a.N1 = a.N2 = (int)num_frames;
+  a.H = ht, a.W = wd, a.M = (int)num_edges, a.r = radius, a.levels = levels;
+  a.info = info;
+  a.poses = poses;
+  a.disps = disps;
+  a.intr = intrinsics;
+  a.num_poses = num_poses;
+  a.num_disps = num_disps;
+  a.coords_out = coords1;
+  int rc;
+  if ((rc = bind_device(corr))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ntiles = ((wd + kAtSide - 1) / kAtSide) * ((ht + kAtSide - 1) / kAtSide);
+  dim3 grid(ntiles, (unsigned)num_edges, levels);
+  HS2_PROF("corr_fused_tile", s);
+  if (dtype == HS2_F16) {
+    if ((rc = at_prepare<__half, true>())) return rc;
+    altcorr_fwd_tile_kernel<__half, true><<<grid, kAtThreads, kAtSmem, s>>>(a);
+  } else {
+    if ((rc = at_prepare<__nv_bfloat16, true>())) return rc;
+    altcorr_fwd_tile_kernel<__nv_bfloat16, true><<<grid, kAtThreads, kAtSmem, s>>>(a);
+  }
+  HS2_LAUNCH_CHECK("altcorr_fwd_tile_kernel (fused)");
+  return HS2_OK;
 }

@@ -2996,10 +2996,16 @@ pg_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float
         }
       }
     }
+    {
+      // the first 32 sums by the transpose exchange (lane l ends with the total of h[l]),
+      // the remaining ones by plain butterflies
+      static_assert(kPgH >= 32, "pg_linearize: at least 32 sums per edge");
 #pragma unroll
-    for (int i = 0; i < kPgH; ++i) {
-      const float v = warp_sum(h[i]);
-      if (lane == 0) red[warp][i] = v;
+      for (int i = 32; i < kPgH; ++i) {
+        const float v = warp_sum(h[i]);
+        if (lane == 0) red[warp][i] = v;
+      }
+      red[warp][lane] = warp_transpose_sum(*reinterpret_cast<float(*)[32]>(h));   // consumes h[0..31]
     }
     __syncthreads();
     if (threadIdx.x < kPgH) {

@@ -192,6 +192,18 @@ int hs2_corr_reproject_lookup(const float* poses, int64_t num_poses, const float
                               int64_t num_edges, int radius, void* corr, float* coords1, int32_t* info,
                               hs2_stream_t stream);
 
+/* The same op on channel-last features (float16 / bfloat16, channels == 128, radius <= 8):
+ * packed_levels[l] are hs2_altcorr_pack buffers of the pooled features [1, num_frames,
+ * (ht>>l)*(wd>>l), 128] (level 0 must hold the frames of ii and jj, the other levels
+ * those of jj).  Each CTA takes an 8x8 block of pixels of one edge and level, reprojects
+ * them (the formula above), and computes the block's windows by the staged-box tensor-core
+ * product of hs2_altcorr_forward_packed; same outputs. */
+int hs2_corr_reproject_lookup_packed(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps,
+                                     const float* intrinsics, const void* const* packed_levels, int levels, int dtype,
+                                     int64_t num_frames, int channels, int ht, int wd, const int64_t* ii,
+                                     const int64_t* jj, int64_t num_edges, int radius, void* corr, float* coords1,
+                                     int32_t* info, hs2_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * altcorr_forward  (reference: src/droid.cpp:277-289, src/altcorr_kernel.cu:25-75,132-172)
  *   fmap1 [b,n1,c,h,w], fmap2 [b,n2,c,h2,w2] of `dtype`, coords [b,m,2,h,w] f32,

@@ -73,3 +73,25 @@ def test_fused_lookup_without_coords_and_bad_index(cuda):
     corr_bad, _ = backends.corr_reproject_lookup(*args, c["ii"], bad, 3)
     torch.cuda.synchronize()
     assert float(corr_bad[0].abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16], ids=["f16", "bf16"])
+def test_fused_packed_path_matches_direct_kernel(cuda, dtype):
+    """16-bit features with 128 channels take the channel-last tensor-core path (8x8-pixel
+    blocks, reprojection in the kernel); it matches the per-tap kernel (only the summation
+    order differs before the output is rounded) and reports an out-of-range edge the same way."""
+    p = synth.make_ba_problem("frontend", seed=2)
+    c = synth.make_corr_problem("frontend", seed=2, device=cuda, dtype=dtype)
+    pyr = levels_of(c["fmaps"])
+    args = (pyr, p["poses"].to(cuda), p["disps"].to(cuda), p["intrinsics"].to(cuda))
+    ii, jj = c["ii"][:40], c["jj"][:40].clone()
+    fast, cf = backends.corr_reproject_lookup(*args, ii, jj, 3)
+    slow, cs = backends.corr_reproject_lookup(*args, ii, jj, 3, path="direct")
+    assert float((cf - cs).abs().max()) < 1e-4
+    tol = 2 ** -10 if dtype == torch.float16 else 2 ** -7
+    assert rel(fast, slow) < tol
+    jj[5] = 1000
+    bad, _ = backends.corr_reproject_lookup(*args, ii, jj, 3)
+    torch.cuda.synchronize()
+    assert float(bad[5].float().abs().max()) == 0.0
+    assert rel(bad[:5], fast[:5]) < tol
