@@ -251,3 +251,24 @@ def test_altcorr_tiled_smooth_coords_vs_oracle(cuda, dtype, level, r):
     assert rel(np64(out), ref) < tol
     direct, = droid_backends.altcorr_forward(f1, f2, crd, ii, jj, r, path="direct")
     assert rel(np64(out), np64(direct)) < tol
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float16, 2 ** -10), (torch.bfloat16, 2 ** -7)])
+@pytest.mark.parametrize("r", [3, 4])
+@pytest.mark.parametrize("integer_frac", [False, True])
+def test_corr_index_16bit_odd_planes(cuda, dtype, tol, r, integer_frac):
+    """16-bit volumes with odd plane sizes and an odd element count (windows starting at
+    either parity, one on the volume's very last element, taps past every border) on the
+    radius-3/4 kernel against the float32 path on the same values."""
+    vol, crd = make_lookup(3, 5, 7, 7, 9, seed=20 + r, dev=cuda, dtype=dtype, integer_frac=integer_frac)
+    assert vol.numel() % 2 == 1
+    out, = droid_backends.corr_index_forward(vol, crd, r)
+    ref32, = droid_backends.corr_index_forward(vol.float(), crd, r)
+    assert rel(np64(out), np64(ref32)) < tol
+    # a window on the very last element of the volume
+    crd2 = crd.clone()
+    crd2[-1, 0, -1, -1] = 8.3
+    crd2[-1, 1, -1, -1] = 6.6
+    out2, = droid_backends.corr_index_forward(vol, crd2, r)
+    ref2, = droid_backends.corr_index_forward(vol.float(), crd2, r)
+    assert rel(np64(out2), np64(ref2)) < tol
