@@ -845,7 +845,7 @@ extern "C" int hs2_altcorr_pack_workspace_size(int dtype, int b, int n, int c, i
     set_error("altcorr_pack: float16 or bfloat16 features only (dtype %d)", dtype);
     return HS2_ERR_DTYPE;
   }
-  if (b < 0 || n < 0 || c <= 0 || c > 256 || h <= 0 || w <= 0) {
+  if (b < 0 || n < 0 || c <= 0 || c > 256 || h <= 0 || w <= 0 || b > 65535 || n > 65535) {
     set_error("altcorr_pack: bad sizes b=%d n=%d c=%d h=%d w=%d", b, n, c, h, w);
     return HS2_ERR_INVALID;
   }

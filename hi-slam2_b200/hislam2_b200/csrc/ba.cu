@@ -1371,6 +1371,11 @@ constexpr int kCholThreads = 256;
 constexpr int kPLD = 66;   // padded row length (doubles) of panel/tile rows in shared memory
 constexpr unsigned kBarrierSpins = 1u << 22;
 constexpr int kCtlFlags = 4;   // ctl[4 + c]: x of block c is final
+// A panel's X tile (the 64 rows of one block row below D) is split over kXSplit tasks of
+// kXRows rows, so the tasks that carry the pivot chain are no longer than the D-only task
+// by a whole tile's solve; each task counts itself on its block row.
+constexpr int kXSplit = 2;
+constexpr int kXRows = 64 / kXSplit;
 
 struct CholBuf {
   double* L11;      // [nbk][64][64] factored diagonal blocks (zero above the diagonal)
@@ -1483,7 +1488,7 @@ __device__ bool chol_wait_tile(const unsigned* lcnt, const unsigned* tcnt, int n
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0)
-    s_ok = wait_count(lcnt + R, kb + 1, info) && wait_count(lcnt + C, kb + 1, info) &&
+    s_ok = wait_count(lcnt + R, kXSplit * (kb + 1), info) && wait_count(lcnt + C, kXSplit * (kb + 1), info) &&
            wait_count(tcnt + (int64_t)R * nbk + C, tdone, info);
   __syncthreads();
   return s_ok != 0;
@@ -1618,12 +1623,12 @@ __device__ __forceinline__ void chol_factor_diag(double (*Pm)[kPLD], double* bv,
 
 // Panel kb, task t (0: D only; t >= 1: D and the (t-1)-th tile below it).  Returns
 // false when a pivot is not positive (ctl[2] is then set).
-__device__ bool chol_panel(int n, int kb, int t, double* __restrict__ A, double* __restrict__ bvec, CholBuf cb,
-                           double* csm) {
+__device__ bool chol_panel(int n, int kb, int t, int xh, double* __restrict__ A, double* __restrict__ bvec,
+                           CholBuf cb, double* csm) {
   const int tid = threadIdx.x;
   const int o = kb * kNB, nb = min(kNB, n - o);
-  const int r0 = o + nb + (t - 1) * kNB;
-  const int nr = t == 0 ? 0 : min(kNB, n - r0);
+  const int r0 = o + nb + (t - 1) * kNB + xh * kXRows;
+  const int nr = t == 0 ? 0 : max(0, min(kXRows, n - r0));
   double (*Pm)[kPLD] = reinterpret_cast<double (*)[kPLD]>(csm);   // [128][kPLD]: D rows, then X rows
   double* bv = csm + 128 * kPLD;                                   // [128]
   double* sv = bv + 128;                                           // [64] 1/L_jj
@@ -1967,8 +1972,11 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
   unsigned* slices = cb.ctl + kCtlFlags + nbk;
   unsigned* lcnt = cb.ctl + kCtlFlags + 2 * nbk;
   unsigned* tcnt = cb.ctl + kCtlFlags + 3 * nbk;
-  for (int t = blockIdx.x; t < nbk; t += G) {
-    chol_panel(n, 0, t, A, bvec, cb, csm);
+  // panel task tau of a panel with `rest` block rows from its diagonal down: tau = 0 is D
+  // alone, tau >= 1 is half (tau - 1) % kXSplit of block row 1 + (tau - 1) / kXSplit
+  for (int tau = blockIdx.x; tau < 1 + kXSplit * (nbk - 1); tau += G) {
+    const int t = tau == 0 ? 0 : 1 + (tau - 1) / kXSplit, xh = tau == 0 ? 0 : (tau - 1) % kXSplit;
+    chol_panel(n, 0, t, xh, A, bvec, cb, csm);
     __syncthreads();
     if (threadIdx.x == 0 && t > 0) red_release_add_gpu(lcnt + t, 1u);
   }
@@ -1990,24 +1998,27 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
     // round-robin over the remaining CTAs.  A panel task counts the L block it writes on
     // its block row; a tile counts the update it applied.
     const int ntiles = rest * (rest - 1) / 2;
-    const bool split = (int)G > rest;
-    const int tfirst = split ? ((int)blockIdx.x < rest ? ntiles : (int)blockIdx.x - rest) : (int)blockIdx.x;
-    const int tstep = split ? (int)G - rest : (int)G;
-    if (split && (int)blockIdx.x < rest) {
-      if (!chol_wait_slices(slices, kb, blockIdx.x, info)) return;
-      chol_panel(n, kb + 1, blockIdx.x, A, bvec, cb, csm);
+    const int ntask = 1 + kXSplit * (rest - 1);
+    const bool split = (int)G > ntask;
+    const int tfirst = split ? ((int)blockIdx.x < ntask ? ntiles : (int)blockIdx.x - ntask) : (int)blockIdx.x;
+    const int tstep = split ? (int)G - ntask : (int)G;
+    auto panel_task = [&](int tau) -> bool {
+      const int t = tau == 0 ? 0 : 1 + (tau - 1) / kXSplit, xh = tau == 0 ? 0 : (tau - 1) % kXSplit;
+      if (!chol_wait_slices(slices, kb, t, info)) return false;
+      chol_panel(n, kb + 1, t, xh, A, bvec, cb, csm);
       __syncthreads();
-      if (threadIdx.x == 0 && blockIdx.x > 0) red_release_add_gpu(lcnt + kb + 1 + blockIdx.x, 1u);
+      if (threadIdx.x == 0 && t > 0) red_release_add_gpu(lcnt + kb + 1 + t, 1u);
+      return true;
+    };
+    if (split && (int)blockIdx.x < ntask) {
+      if (!panel_task(blockIdx.x)) return;
     }
-    for (int t = tfirst; t < (split ? ntiles : rest + ntiles); t += tstep) {
-      if (!split && t < rest) {
-        if (!chol_wait_slices(slices, kb, t, info)) return;
-        chol_panel(n, kb + 1, t, A, bvec, cb, csm);
-        __syncthreads();
-        if (threadIdx.x == 0 && t > 0) red_release_add_gpu(lcnt + kb + 1 + t, 1u);
+    for (int t = tfirst; t < (split ? ntiles : ntask + ntiles); t += tstep) {
+      if (!split && t < ntask) {
+        if (!panel_task(t)) return;
         continue;
       }
-      int I = 0, tt = split ? t : t - rest;
+      int I = 0, tt = split ? t : t - ntask;
       while (tt > I) {
         tt -= I + 1;
         ++I;
