@@ -2074,7 +2074,7 @@ __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restr
       xs[i / 6][i % 6] = (ix <= 0 || ix >= P) ? 0.f : dx[ix * 6 + i % 6];
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll 8
     for (int i = 0; i < nrw; ++i) {
       const int ix = w.rpose[rb + i];
       if (ix <= 0 || ix >= P) continue;
