@@ -2855,9 +2855,15 @@ namespace hs2 {
 constexpr int kPgD = 7;
 constexpr int kPgTab = 72;        // floats per edge: t 0..2, q 3..6, s 7, L 8..56 (row-major), s R 57..65
 constexpr int kPgH = 35;          // upper triangle of Hjj (28), then vj (7)
-constexpr int kPgThreads = 256;
+// pg_linearize: 128 threads x 4 pixels (four CTAs per SM); pg_backsub: 256 threads x 2
+// pixels over the same 512-pixel chunks (measured: 0.63 / 0.16 ms at 300 kf against
+// 0.67 / 0.20 ms with 256 x 4 for both)
+constexpr int kPgThreads = 128;
 constexpr int kPgPPT = 4;
 constexpr int kPgChunk = kPgThreads * kPgPPT;
+constexpr int kPgBsThreads = 256;
+constexpr int kPgBsPPT = 2;
+static_assert(kPgBsThreads * kPgBsPPT == kPgChunk, "pg_backsub covers the linearisation's chunks");
 constexpr int kPgSplit = 16;      // CTAs per depth frame in the Gram
 
 __host__ __device__ __forceinline__ int64_t pg_order(int P) { return 7 * (int64_t)P + ((7 * (int64_t)P) & 1); }
@@ -2910,10 +2916,10 @@ __global__ void pg_edge_kernel(const float* __restrict__ poses, const int64_t* _
 }
 
 // One CTA per (depth frame slot, chunk of kPgChunk pixels); thread t owns the pixels
-// t + 256 k.  For every edge of the frame (in group order) each pixel is moved by
+// t + kPgThreads k.  For every edge of the frame (in group order) each pixel is moved by
 // Gij, projected and linearised as the reference does per pixel (:700-814); the
 // edge's 35 Hessian sums are reduced over the CTA into FP64 accumulators.
-__global__ void __launch_bounds__(kPgThreads)
+__global__ void __launch_bounds__(kPgThreads, 4)
 pg_linearize_kernel(const float* __restrict__ disps, int HW, int wd, const float* __restrict__ intr,
                     const float* __restrict__ targets, const float* __restrict__ weights,
                     const float* __restrict__ eta, int64_t eta_rows, const int64_t* __restrict__ jj, int t0,
@@ -3233,7 +3239,7 @@ pg_schur_rhs_kernel(int HW, BaPtrs w, const float* __restrict__ erows, const flo
 
 // dz = Q (w - sum_rows E.dx[pose]) over the frame's rows whose pose index lies in
 // (0, P) (EvT6x1_kernel :1562-1582 skips ix <= 0), disps[kx] += dz (:1398-1411).
-__global__ void __launch_bounds__(kPgThreads)
+__global__ void __launch_bounds__(kPgBsThreads)
 pg_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const float* __restrict__ erows,
                   const float* __restrict__ qbuf, const float* __restrict__ wbuf, const float* __restrict__ dx,
                   float* __restrict__ dz, const int32_t* __restrict__ info) {
@@ -3245,8 +3251,8 @@ pg_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const floa
   const int f = w.kx[s];
   const int base = blockIdx.y * kPgChunk + threadIdx.x;
 #pragma unroll
-  for (int k = 0; k < kPgPPT; ++k) {
-    const int p = base + k * kPgThreads;
+  for (int k = 0; k < kPgBsPPT; ++k) {
+    const int p = base + k * kPgBsThreads;
     if (p >= HW) continue;
     float acc = 0.f;
     for (int r = r0; r < r1; ++r) {
@@ -3445,7 +3451,7 @@ extern "C" int hs2_pgba(const float* poses, int64_t num_poses, float* disps, int
   }
   if (S > 0) {
     HS2_PROF("pg_backsub", s);
-    pg_backsub_kernel<<<dim3((unsigned)S, nchunk), kPgThreads, 0, s>>>(disps, p.HW, P, w, erows, qbuf, wbuf, dxf,
+    pg_backsub_kernel<<<dim3((unsigned)S, nchunk), kPgBsThreads, 0, s>>>(disps, p.HW, P, w, erows, qbuf, wbuf, dxf,
                                                                        dz, info);
     HS2_LAUNCH_CHECK("pg_backsub_kernel");
   }
