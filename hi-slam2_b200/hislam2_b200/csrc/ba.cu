@@ -2046,11 +2046,11 @@ ba_cholesky_kernel(int n, float lm, float ep, BaPtrs w, CholBuf cb, float* __res
 }
 
 // -------------------------------------------------------------- backsub ---
-template <int NT>
+template <int NT, int PPT = kLinPPT>
 __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restrict__ disps, int HW, int P, BaPtrs w,
                                                 const float* __restrict__ dx, float* __restrict__ dz,
                                                 int64_t dz_rows, const int32_t* __restrict__ info) {
-  constexpr int kChunk = NT * kLinPPT;
+  constexpr int kChunk = NT * PPT;
   if (info[0]) return;
   if (s >= info[1] || s >= dz_rows) return;
   const int f = w.kx[s];
@@ -2058,10 +2058,10 @@ __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restr
   const int HWs = row_stride(HW);
   constexpr int kRows = 64;                 // rows whose dx sit in shared memory at a time
   __shared__ float xs[kRows][6];
-  float acc[kLinPPT];
-  int pix[kLinPPT];
+  float acc[PPT];
+  int pix[PPT];
 #pragma unroll
-  for (int k = 0; k < kLinPPT; ++k) {
+  for (int k = 0; k < PPT; ++k) {
     pix[k] = chunk * kChunk + k * NT + threadIdx.x;
     acc[k] = 0.f;
   }
@@ -2080,7 +2080,7 @@ __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restr
       if (ix <= 0 || ix >= P) continue;
       const float* Er = w.erows + ((int64_t)(rb + i) * 6) * HWs;
 #pragma unroll
-      for (int k = 0; k < kLinPPT; ++k) {
+      for (int k = 0; k < PPT; ++k) {
         const int p = pix[k];
         if (p >= HW) continue;
         float d = 0.f;
@@ -2091,7 +2091,7 @@ __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restr
     }
   }
 #pragma unroll
-  for (int k = 0; k < kLinPPT; ++k) {
+  for (int k = 0; k < PPT; ++k) {
     const int p = pix[k];
     if (p >= HW) continue;
     const int64_t o = (int64_t)s * HW + p;
@@ -2101,10 +2101,16 @@ __device__ __forceinline__ void ba_backsub_body(int s, int chunk, float* __restr
   }
 }
 
-__global__ void __launch_bounds__(kLinThreads)
+// 256 threads x 2 pixels over the linearisation's 512-pixel chunks (measured at 300 kf:
+// 0.094 ms against 0.107 ms with 128 x 4)
+constexpr int kBsThreads = 2 * kLinThreads;
+constexpr int kBsPPT = kLinPPT / 2;
+static_assert(kBsThreads * kBsPPT == kLinChunk, "back-substitution covers the linearisation's chunks");
+
+__global__ void __launch_bounds__(kBsThreads)
 ba_backsub_kernel(float* __restrict__ disps, int HW, int P, BaPtrs w, const float* __restrict__ dx,
                   float* __restrict__ dz, int64_t dz_rows, const int32_t* __restrict__ info) {
-  ba_backsub_body<kLinThreads>(blockIdx.x, blockIdx.y, disps, HW, P, w, dx, dz, dz_rows, info);
+  ba_backsub_body<kBsThreads, kBsPPT>(blockIdx.x, blockIdx.y, disps, HW, P, w, dx, dz, dz_rows, info);
 }
 
 // ------------------------------------------------------------ pose retr ---
@@ -2418,7 +2424,7 @@ extern "C" int hs2_ba(float* poses, int64_t num_poses, float* disps, int64_t num
                                                              dx, dz, dz_rows, info);
         HS2_LAUNCH_CHECK("ba_backsub_frame_kernel");
       } else {
-        ba_backsub_kernel<<<grid, kLinThreads, 0, s>>>(disps, p.HW, P, w, dx, dz, dz_rows, info);
+        ba_backsub_kernel<<<grid, kBsThreads, 0, s>>>(disps, p.HW, P, w, dx, dz, dz_rows, info);
         HS2_LAUNCH_CHECK("ba_backsub_kernel");
       }
     }
