@@ -216,3 +216,48 @@ def test_gram_precision_setter_validation():
     assert lib.hs2_ba_set_gram_precision(2) == _lib.HS2_ERR_INVALID
     assert b"3xTF32" in lib.hs2_last_error()
     assert lib.hs2_ba_set_gram_precision(1) == _lib.HS2_OK
+
+
+def test_packed_altcorr_host_validation():
+    """The channel-last correlation entry points refuse bad arguments before any launch."""
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.hs2_altcorr_pack_workspace_size(_lib.HS2_F32, 1, 4, 128, 8, 9, ctypes.byref(n)) == _lib.HS2_ERR_DTYPE
+    assert lib.hs2_altcorr_pack_workspace_size(_lib.HS2_F16, 1, 4, 300, 8, 9, ctypes.byref(n)) == _lib.HS2_ERR_INVALID
+    assert lib.hs2_altcorr_pack_workspace_size(_lib.HS2_F16, 1, 4, 128, 8, 9, ctypes.byref(n)) == _lib.HS2_OK
+    assert n.value >= 4 * 8 * 9 * 128 * 2 + 4                   # packed rows + one flag byte per frame
+    assert lib.hs2_altcorr_pack(None, _lib.HS2_F16, 1, 4, 128, 8, 9, None, 0, None, 0, None) == \
+        _lib.HS2_ERR_WORKSPACE
+    assert lib.hs2_altcorr_pack(None, _lib.HS2_F16, 1, 4, 128, 8, 9, None, 3, 1, n.value, None) == \
+        _lib.HS2_ERR_INVALID                                     # a frame count without a frame list
+    assert lib.hs2_altcorr_pack(None, _lib.HS2_BF16, 0, 4, 128, 8, 9, None, 0, 1, n.value, None) == _lib.HS2_OK
+    fwd = [1, 1, _lib.HS2_F16, 1, 4, 4, 128, 8, 9, 4, 5, 1, 1, 1, 3, 3, 1, 1, None]
+    f32 = list(fwd)
+    f32[2] = _lib.HS2_F32
+    assert lib.hs2_altcorr_forward_packed(*f32) == _lib.HS2_ERR_DTYPE
+    neg = list(fwd)
+    neg[6] = 0
+    assert lib.hs2_altcorr_forward_packed(*neg) == _lib.HS2_ERR_INVALID
+    empty = list(fwd)
+    empty[14] = 0
+    assert lib.hs2_altcorr_forward_packed(*empty) == _lib.HS2_OK
+
+
+def test_fused_packed_lookup_host_validation():
+    lib = _lib.load()
+    ptrs = (ctypes.c_void_p * 4)(1, 1, 1, 1)
+    args = [1, 10, 1, 10, 1, ptrs, 4, _lib.HS2_F16, 10, 128, 43, 77, 1, 1, 20, 3, 1, None, 1, None]
+    for idx, val, rc in ((9, 64, _lib.HS2_ERR_INVALID),       # 128 channels only
+                         (15, 9, _lib.HS2_ERR_INVALID),       # radius <= 8
+                         (7, _lib.HS2_F32, _lib.HS2_ERR_DTYPE),
+                         (6, 0, _lib.HS2_ERR_INVALID)):
+        bad = list(args)
+        bad[idx] = val
+        assert lib.hs2_corr_reproject_lookup_packed(*bad) == rc, (idx, val)
+    missing = list(args)
+    missing[5] = (ctypes.c_void_p * 4)(1, 0, 1, 1)
+    assert lib.hs2_corr_reproject_lookup_packed(*missing) == _lib.HS2_ERR_INVALID
+    assert b"level 1" in lib.hs2_last_error()
+    empty = list(args)
+    empty[14] = 0
+    assert lib.hs2_corr_reproject_lookup_packed(*empty) == _lib.HS2_OK
