@@ -21,7 +21,8 @@
 //                  frame read as zero) with 3-D TMA boxes (128B swizzle) into a
 //                  2-stage ring; warp 1 issues tcgen05.mma (kind::f16 for F16/BF16,
 //                  kind::f8f6f4 for E4M3; M = 128, N = 2 RW, accumulator F32) into
-//                  one of two 256-column TMEM buffers; warps 2-9 drain the
+//                  one of two 256-column TMEM buffers; warps 2-17 (four per TMEM
+//                  lane quarter, each half an image row of the tile) drain the
 //                  accumulator (tcgen05.ld), round to the volume type into a
 //                  shared staging tile, write level 0 in 16-byte chunks aligned in
 //                  global memory, pool level 1 from the two rows of the tile, and
