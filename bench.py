@@ -350,6 +350,7 @@ def run_ours(args, world, rank, local):
     step = backend_step_leg(args, dev, world)
     vol = volume_leg(args, dev, world, peaks) if world == 1 else None
     bat = batch_leg(args, dev, world, rank)
+    jd = jdsa_leg(args, dev, world, rank)
 
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = json.load(open(traffic_path)) if os.path.exists(traffic_path) else {}
@@ -368,7 +369,7 @@ def run_ours(args, world, rank, local):
                 "config": dict(CONFIG, parallelism="replicas: one independent window per rank" if world > 1 else
                                "single GPU"),
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu,
-                "accuracy": acc, "corr_lookup": corr, "altcorr": alt, "backend_step": step, "corr_volume": vol, "batch": bat, "pgba": pg, "clocks": clk,
+                "accuracy": acc, "corr_lookup": corr, "altcorr": alt, "backend_step": step, "corr_volume": vol, "batch": bat, "pgba": pg, "jdsa": jd, "clocks": clk,
                 "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
                 "library_peaks_tflops": {"sgemm_fp32": round(simt[0], 2), "dgemm_fp64": round(simt[1], 2)}}
         print(json.dumps(line), flush=True)
@@ -719,6 +720,43 @@ def pgba_leg(args, dev, world, rank):
     torch.cuda.empty_cache()
     return {"value": round(world * 1e3 / ms, 2), "unit": "pgba steps/s", "ms_per_step": round(ms, 4),
             "config": "backend300 window with Sim3 poses, 600 relative-pose factors, one GN step",
+            "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())}}
+
+
+def jdsa_leg(args, dev, world, rank):
+    """The mono-prior alignment step (hislam2_b200.mono.JDSA, one hs2_jdsa call: proj_trans
+    plus the per-frame scale solve and depth update) on HI-SLAM2's frontend window, 25
+    keyframes at 43x77 with 258 edges and its 2x2 scale grid per frame, device-timed."""
+    from hislam2_b200 import _lib, mono, replicas, synth
+
+    g = synth.make_jdsa_problem("frontend", seed=replicas.window_seed(rank), device=dev)
+    init = g["dscales"].clone()
+    dscales = init.clone()
+    disps = g["disps"][None]
+
+    def step():
+        dscales.copy_(init)
+        mono.JDSA(g["targets"], g["weights"], g["eta"], g["poses"], disps, g["intrinsics"], g["disps_prior"],
+                  dscales, g["ii"], g["jj"], g["alpha"])
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    _lib.profile_report(reset=True)
+    _lib.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    _lib.profile_enable(False)
+    prof = _lib.profile_report(reset=True)
+    ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.steps
+    return {"value": round(world * 1e3 / ms, 2), "unit": "JDSA steps/s", "ms_per_step": round(ms, 4),
+            "config": "frontend window: 25 kf, 43x77, 258 edges, 2x2 scale grid, alpha 0.01; the step's "
+                      "host sync (torch.unique, info read) included",
             "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())}}
 
 

@@ -17,6 +17,7 @@ HS2_DEV_BAD_INDEX = 1
 HS2_DEV_BAD_ETA = 2
 HS2_DEV_TIMEOUT = 4
 HS2_DEV_LIMIT = 8
+HS2_DEV_NOT_PD = 16
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int
@@ -62,6 +63,8 @@ SIGNATURES = {
     "hs2_iproj": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p],
     "hs2_proj_trans": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _p, _i64, _i64, _p, _p, _p, _p],
     "hs2_bi_inter": [_p, _i64, _i32, _i32, _p, _i32, _i32, _p, _p, _p, _p],
+    "hs2_jdsa": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p,
+                 _i64, _p, _i64, _f32, _p, _p, _p, _p, _p, _p, _p],
     "hs2_covis_distance": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _p],
     "hs2_depth_filter": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _i64, _p, _p, _p],
     "hs2_profile_enable": [_i32],

@@ -281,3 +281,38 @@ def make_batch_problems(num_windows=64, seed=0, device="cpu"):
                         eta=torch.full((K, ht, wd), 1e-3, **f32), ii=ii.to(device), jj=jj.to(device), t0=t0, t1=K,
                         iters=4, lm=1e-4, ep=0.1))
     return out
+
+
+def make_jdsa_problem(name="tiny6", seed=0, device="cpu", hs=2, ws=2, alpha=0.01, keep=None,
+                      prior_holes=0.1):
+    """Inputs of the mono-prior alignment step ``JDSA`` (``hislam2/geom/ba.py:170``) for the
+    BA workload ``name``: its poses, disparities, targets and weights; the edges whose
+    source frame passes ``keep`` (default all); ``disps_prior`` [K,H,W] = ground truth
+    divided by a smooth per-frame scale field (1 + 0.2 N(0,1) at 3x3 control points,
+    bilinear), times 1 + 0.02 N(0,1), with a fraction ``prior_holes`` of pixels set to 0
+    (no prior); ``dscales`` [t1,hs,ws] = 1 + 0.05 N(0,1); eta [M,H,W] = 0.2 U[0,1e-2] +
+    1e-7 for the M = len(unique(ii)) source frames (the caller's ``.2 * damping + EP``).
+    ``alpha`` is ``mono_depth_alpha`` (0.01 in most of HI-SLAM2's configs)."""
+    p = make_ba_problem(name, seed=seed, device="cpu")
+    g = torch.Generator().manual_seed(seed + 4000)
+    K, ht, wd = p["disps"].shape
+    t1 = p["t1"]
+    ii, jj = p["ii"], p["jj"]
+    if keep is not None:
+        sel = torch.tensor([bool(keep(int(i))) for i in ii])
+        ii, jj = ii[sel], jj[sel]
+        p["targets"], p["weights"] = p["targets"][sel].contiguous(), p["weights"][sel].contiguous()
+    ctrl = 1.0 + 0.2 * torch.randn(K, 1, 3, 3, generator=g, dtype=torch.float64)
+    field = torch.nn.functional.interpolate(ctrl, size=(ht, wd), mode="bilinear", align_corners=True)[:, 0]
+    prior = p["disps_gt"].double() / field.clamp(min=0.3)
+    prior = prior * (1.0 + 0.02 * torch.randn(K, ht, wd, generator=g, dtype=torch.float64))
+    prior = torch.where(torch.rand(K, ht, wd, generator=g) < prior_holes, torch.zeros_like(prior), prior)
+    dscales = 1.0 + 0.05 * torch.randn(t1, hs, ws, generator=g, dtype=torch.float64)
+    M = int(torch.unique(ii).numel())
+    eta = 0.2 * 1e-2 * torch.rand(M, ht, wd, generator=g, dtype=torch.float64) + 1e-7
+    f32 = dict(dtype=torch.float32, device=device)
+    return dict(targets=p["targets"].to(device), weights=p["weights"].to(device), eta=eta.to(**f32),
+                poses=p["poses"][:t1].contiguous().to(device), disps=p["disps"][:t1].contiguous().to(device),
+                intrinsics=p["intrinsics"].to(device), disps_prior=prior.to(**f32).contiguous(),
+                dscales=dscales.to(**f32).contiguous(), ii=ii.contiguous().to(device),
+                jj=jj.contiguous().to(device), alpha=float(alpha))

@@ -40,7 +40,8 @@ enum hs2_device_error {
   HS2_DEV_BAD_INDEX = 1, /* an edge index lies outside the pose/disparity buffers or >= t1 */
   HS2_DEV_BAD_ETA = 2,   /* eta has neither M nor 1 rows (M = #distinct depth frames) */
   HS2_DEV_TIMEOUT = 4,   /* a bounded wait inside a kernel gave up (results are not valid) */
-  HS2_DEV_LIMIT = 8      /* a per-kernel size limit was exceeded (results are not valid) */
+  HS2_DEV_LIMIT = 8,     /* a per-kernel size limit was exceeded (results are not valid) */
+  HS2_DEV_NOT_PD = 16    /* a system to be factorised was not positive definite (hs2_jdsa) */
 };
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -395,6 +396,35 @@ int hs2_proj_trans(const float* poses, int64_t num_poses, const float* disps, in
  */
 int hs2_bi_inter(const float* scales, int64_t num, int hs, int ws, const float* grids, int ht, int wd,
                  float* outputs, float* jacobians, int32_t* info, hs2_stream_t stream);
+
+/* jdsa  (reference: hislam2/geom/ba.py:170-219 JDSA, :159-167 get_prior_depth_aligned,
+ *        hislam2/geom/chol.py:80-107 schur_solve_mono_prior; the caller is
+ *        hislam2/depth_video.py:234-240)
+ * One mono-prior depth / scale alignment step after ba: proj_trans's C, w of the edges
+ * (ii, jj), the prior terms of disps_prior [num_prior, H, W] aligned by the per-frame
+ * bilinear scale grids dscales [num_scales, hs, ws], a damped solve (ep 0.1, lm 1e-4) for
+ * the hs*ws scale unknowns of every source frame and the depth update by back-substitution.
+ *   disps [num_disps, H, W] is read only; disps_out [num_disps, H, W] receives
+ *   clamp(where(d > 10, 0, d), min = 0.001) of every frame, d = disps + dz on the source
+ *   frames.  dscales[kx[b]] += dso[b] in place.  dso [M, hs*ws] and dzcov [M, H*W] (may be
+ *   NULL) are outputs; C, w [M, H*W] are scratch.  M = num_kx.
+ *   kx [M]: the sorted distinct values of ii; slot [num_edges]: the position of ii[e] in kx
+ *   (torch.unique(ii, return_inverse=True)).  eta: M*H*W values (row b for frame kx[b]).
+ *   grid_y [ht] = linspace(0, hs-1-1e-6, ht), grid_x [wd] = linspace(0, ws-1-1e-6, wd), in
+ *   float32 as torch.linspace computes them (the reference's sampling grid).
+ *   Limits: 2 <= hs, ws; hs*ws <= 16; ht, wd <= 4096; 1 <= M <= 65535.
+ *   info: int32[1], zeroed here; HS2_DEV_BAD_INDEX for an edge or kx outside the buffers, an
+ *   unsorted kx or a grid point whose 2x2 cell leaves the scale grid; HS2_DEV_NOT_PD when a
+ *   block of the reduced system is not positive definite (the reference raises there, in
+ *   torch.linalg.inv of the zero factor its CholeskySolver returns).  With either bit set
+ *   dscales is left unchanged and disps_out is not valid.
+ */
+int hs2_jdsa(const float* poses, int64_t num_poses, const float* disps, int64_t num_disps, int ht, int wd,
+             const float* intrinsics, const float* targets, const float* weights, const float* eta,
+             const float* disps_prior, int64_t num_prior, float* dscales, int64_t num_scales, int hs, int ws,
+             const float* grid_y, const float* grid_x, const int64_t* ii, const int64_t* jj, const int64_t* slot,
+             int64_t num_edges, const int64_t* kx, int64_t num_kx, float alpha, float* C, float* w, float* dso,
+             float* disps_out, float* dzcov, int32_t* info, hs2_stream_t stream);
 
 /* Selects the kernels of the linearisation and Schur Gram for later hs2_ba calls
  * (process-wide; no counterpart in the reference, whose Gram is SIMT FP32 in

@@ -261,3 +261,30 @@ def test_fused_packed_lookup_host_validation():
     empty = list(args)
     empty[14] = 0
     assert lib.hs2_corr_reproject_lookup_packed(*empty) == _lib.HS2_OK
+
+
+def test_jdsa_host_validation():
+    """hs2_jdsa refuses sizes outside its limits and missing buffers before any launch."""
+    lib = _lib.load()
+    args = [1, 6, 1, 6, 12, 16, 1, 1, 1, 1, 1, 6, 1, 6, 2, 2, 1, 1, 1, 1, 1, 22, 1, 6, 0.01, 1, 1, 1, 1, None, 1, None]
+    for idx, val, what in ((14, 1, b"hs"),                 # a 2x2 cell needs hs, ws >= 2
+                           (15, 9, b"hs*ws"),              # 2 x 9 = 18 scale unknowns > 16
+                           (4, 5000, b"ht"),               # grid axes staged in shared memory
+                           (23, 0, b"source frames"),      # the reference indexes kx[0]
+                           (23, 23, b"source frames"),     # more source frames than edges
+                           (16, None, b"null"),            # grid_y
+                           (27, None, b"null")):           # dso
+        bad = list(args)
+        bad[idx] = val
+        assert lib.hs2_jdsa(*bad) == _lib.HS2_ERR_INVALID, (idx, val)
+        assert what in lib.hs2_last_error(), (idx, lib.hs2_last_error())
+
+
+def test_jdsa_wrapper_checks_inputs_on_cpu():
+    from hislam2_b200 import mono
+    p = {k: torch.zeros(1) for k in ("target", "weight", "eta", "poses", "disps", "intrinsics", "disps_prior",
+                                     "dscales")}
+    ii = torch.zeros(1, dtype=torch.int64)
+    with pytest.raises(RuntimeError, match="CUDA tensor"):
+        mono.JDSA(p["target"], p["weight"], p["eta"], torch.zeros(2, 7), torch.zeros(1, 2, 4, 4),
+                  torch.zeros(4), torch.zeros(2, 4, 4), torch.ones(2, 2, 2), ii, ii, 0.01)
