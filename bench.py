@@ -716,11 +716,25 @@ def pgba_leg(args, dev, world, rank):
     _lib.profile_enable(False)
     prof = _lib.profile_report(reset=True)
     ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / args.steps
+
+    # the rest of DepthVideo.cuda_pgba's iteration: the 600 factors' blocks (numeric Sim3
+    # Jacobians) before the step and the Sim3 retraction of the window after it
+    from hislam2_b200 import pgo
+    rel, infos = synth.make_pgo_factors(g["poses"], g["iip"], g["jjp"], seed=replicas.window_seed(rank))
+    poses = g["poses"].clone()
+    dx = torch.zeros(g["t1"] - g["t0"], 7, device=dev)
+    cons = lambda: pgo.global_relative_posesim3_constraints(g["iip"], g["jjp"], poses, rel, infos, pw=1e-3)  # noqa
+    retr = lambda: pgo.sim3_retr_(poses, dx, g["t0"], g["t1"])  # noqa: E731
+    ms_cons = device_time(cons, args.steps)
+    ms_retr = device_time(retr, args.steps)
     del g, init, disps
     torch.cuda.empty_cache()
     return {"value": round(world * 1e3 / ms, 2), "unit": "pgba steps/s", "ms_per_step": round(ms, 4),
             "config": "backend300 window with Sim3 poses, 600 relative-pose factors, one GN step",
-            "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())}}
+            "kernel_ms_per_step": {k: round(v[1] / args.steps, 4) for k, v in sorted(prof.items())},
+            "pgo_constraints_ms": round(ms_cons, 4), "sim3_retr_ms": round(ms_retr, 4),
+            "loop_note": "one cuda_pgba iteration = pgo_constraints + pgba step + sim3_retr; the "
+                         "constraints time includes its info read (one host sync)"}
 
 
 def jdsa_leg(args, dev, world, rank):

@@ -63,6 +63,8 @@ SIGNATURES = {
     "hs2_iproj": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p],
     "hs2_proj_trans": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _p, _i64, _i64, _p, _p, _p, _p],
     "hs2_bi_inter": [_p, _i64, _i32, _i32, _p, _i32, _i32, _p, _p, _p, _p],
+    "hs2_pgo_constraints": [_p, _i64, _p, _p, _p, _p, _i64, ctypes.c_double, _p, _p, _p, _p, _p],
+    "hs2_sim3_retr": [_p, _i64, _p, _i64, _i64, _p],
     "hs2_jdsa": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p, _i64, _p, _i64, _i32, _i32, _p, _p, _p, _p, _p,
                  _i64, _p, _i64, _f32, _p, _p, _p, _p, _p, _p, _p],
     "hs2_covis_distance": [_p, _i64, _p, _i64, _i32, _i32, _p, _p, _i64, _p, _p, _p],

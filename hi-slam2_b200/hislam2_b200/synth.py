@@ -316,3 +316,25 @@ def make_jdsa_problem(name="tiny6", seed=0, device="cpu", hs=2, ws=2, alpha=0.01
                 intrinsics=p["intrinsics"].to(device), disps_prior=prior.to(**f32).contiguous(),
                 dscales=dscales.to(**f32).contiguous(), ii=ii.contiguous().to(device),
                 jj=jj.contiguous().to(device), alpha=float(alpha))
+
+
+def make_pgo_factors(poses, iip, jjp, seed=0, noise=0.02):
+    """Relative-pose factors between Sim3 poses [K, 8] for the pairs (iip, jjp), in the form
+    ``hislam2/depth_video.py:250-256`` passes them to ``global_relative_posesim3_constraints``:
+    rel_poses [Np, 7] = the SE3 part (t, q) of Gj Gi^-1, moved by an se3 perturbation
+    N(0, noise) so the factors are not at their optimum, and infos [Np, 7, 7] =
+    diag(1 / cov, min(1 / cov)) with cov = 10^-U[1, 4] per translational / rotational axis
+    (the reference appends the smallest information for the scale)."""
+    g = torch.Generator().manual_seed(seed + 5000)
+    P = poses.double().cpu()
+    pi, pj = P[iip.cpu()], P[jjp.cpu()]
+    qi_inv = torch.cat([-pi[:, 3:6], pi[:, 6:7]], -1)
+    q = quat_mul(pj[:, 3:7], qi_inv)
+    t = pj[:, :3] - (pj[:, 7:8] / pi[:, 7:8]) * quat_rotate(q, pi[:, :3])
+    rel = pose_compose(se3_exp(noise * torch.randn(len(iip), 6, generator=g, dtype=torch.float64)),
+                       torch.cat([t, q], -1))
+    Np = len(iip)
+    inv_cov = 10.0 ** (1 + 3 * torch.rand(Np, 6, generator=g, dtype=torch.float64))
+    d = torch.cat([inv_cov, inv_cov.min(1, keepdim=True)[0]], 1)
+    infos = torch.diag_embed(d)
+    return rel.float().to(poses.device).contiguous(), infos.float().to(poses.device).contiguous()

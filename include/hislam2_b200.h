@@ -426,6 +426,30 @@ int hs2_jdsa(const float* poses, int64_t num_poses, const float* disps, int64_t 
              int64_t num_edges, const int64_t* kx, int64_t num_kx, float alpha, float* C, float* w, float* dso,
              float* disps_out, float* dzcov, int32_t* info, hs2_stream_t stream);
 
+/* pgo_constraints  (reference: hislam2/pgo_buffer.py:39-63 global_relative_posesim3_constraints,
+ *                   called at hislam2/depth_video.py:259 before every pgba step)
+ * Blocks of the relative Sim3 pose factors for hs2_pgba: per factor n, the residual
+ * r = log(Gij Gi Gj^-1) with Gi = poses[ii[n]], Gj = poses[jj[n]] (Sim3 [t, q xyzw, s]) and
+ * Gij = rel_poses[n] (SE3 [t, q], scale 1), its Jacobians w.r.t. exp(d) Gi and exp(d) Gj
+ * by central differences of step 1e-8 in FP64 (the reference's numeric Jacobians), then
+ * wJx^T = float((pw Jx)^T info) and
+ *   Hsp [4, num_factors, 7, 7] = [wJi^T Ji, wJi^T Jj, wJj^T Ji, wJj^T Jj],
+ *   vsp [2, num_factors, 7] = -[wJi^T r, wJj^T r],  chi [num_factors, 2] = (r.r, r.info r)
+ * in float32 (sum chi over the factors for the reference's chi2 / chi2_scaled).
+ *   infos [num_factors, 7, 7] f32.  info: int32[1], zeroed here; HS2_DEV_BAD_INDEX for a
+ *   factor whose ii / jj is outside [0, num_poses) (its blocks are zero).
+ */
+int hs2_pgo_constraints(const float* poses, int64_t num_poses, const int64_t* ii, const int64_t* jj,
+                        const float* rel_poses, const float* infos, int64_t num_factors, double pw, float* Hsp,
+                        float* vsp, float* chi, int32_t* info, hs2_stream_t stream);
+
+/* sim3_retr  (reference: hislam2/geom/ba.py:27-29 pose_retr on Sim3 poses, lietorch's retr;
+ *             called at hislam2/depth_video.py:267 after every pgba step)
+ * poses[t0 + k] <- exp(dx[k]) poses[t0 + k] for k < t1 - t0, in place; poses [num_poses, 8]
+ * Sim3 f32, dx [t1 - t0, 7] f32 (pgba's dx).  Computed in FP64, stored as float.
+ */
+int hs2_sim3_retr(float* poses, int64_t num_poses, const float* dx, int64_t t0, int64_t t1, hs2_stream_t stream);
+
 /* Selects the kernels of the linearisation and Schur Gram for later hs2_ba calls
  * (process-wide; no counterpart in the reference, whose Gram is SIMT FP32 in
  * EEt6x6_kernel):

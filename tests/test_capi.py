@@ -288,3 +288,15 @@ def test_jdsa_wrapper_checks_inputs_on_cpu():
     with pytest.raises(RuntimeError, match="CUDA tensor"):
         mono.JDSA(p["target"], p["weight"], p["eta"], torch.zeros(2, 7), torch.zeros(1, 2, 4, 4),
                   torch.zeros(4), torch.zeros(2, 4, 4), torch.ones(2, 2, 2), ii, ii, 0.01)
+
+
+def test_pgo_host_validation():
+    lib = _lib.load()
+    assert lib.hs2_pgo_constraints(1, -1, 1, 1, 1, 1, 4, 1e-3, 1, 1, 1, 1, None) == _lib.HS2_ERR_INVALID
+    assert lib.hs2_pgo_constraints(1, 8, 1, 1, 1, 1, -2, 1e-3, 1, 1, 1, 1, None) == _lib.HS2_ERR_INVALID
+    assert lib.hs2_pgo_constraints(1, 8, 1, 1, 1, 1, 4, 1e-3, 1, 1, 1, None, None) == _lib.HS2_ERR_INVALID
+    assert b"info" in lib.hs2_last_error()
+    assert lib.hs2_sim3_retr(1, 8, 1, 2, 9, None) == _lib.HS2_ERR_INVALID      # t1 beyond the poses
+    assert lib.hs2_sim3_retr(1, 8, 1, 5, 4, None) == _lib.HS2_ERR_INVALID      # t1 < t0
+    assert b"window" in lib.hs2_last_error()
+    assert lib.hs2_sim3_retr(None, 8, None, 3, 3, None) == _lib.HS2_OK         # empty window: nothing to do
