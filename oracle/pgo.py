@@ -19,7 +19,9 @@ are central differences with step 1e-8; here the derivative is taken with a five
 stencil of step 1e-4 on the same function (truncation ~1e-16, rounding ~1e-11), i.e. the
 quantity the reference's differences approximate.  The group conventions are pinned by
 identities in ``tests/test_oracle_pgo.py`` (exp/log inverse pairs, Ji = Ad(Gij) and
-Jj = -I at a zero residual); against lietorch itself the parity is unpinned.
+Jj = -I at a zero residual), and the procedure around them by the reference's own
+``num_jacobi`` / ``global_relative_posesim3_constraints`` run on a Sim3 stand-in
+(``tests/golden/make_golden_pgo.py``); against lietorch itself the parity is unpinned.
 """
 
 import numpy as np

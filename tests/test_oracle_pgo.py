@@ -1,6 +1,7 @@
-"""The pose-graph oracle (``oracle/pgo.py``) pinned by Sim3 identities, and the FP64 Sim3 code
-that ``csrc/pgo.cu`` runs on the device (``csrc/sim3.cuh``, compiled here for the host by
-``tests/sim3_host_harness.cpp``) checked against it on the CPU."""
+"""The pose-graph oracle (``oracle/pgo.py``) pinned by Sim3 identities and by the reference's
+own factor procedure (``tests/golden/pgo_*.npz``), and the FP64 Sim3 code that
+``csrc/pgo.cu`` runs on the device (``csrc/sim3.cuh``, compiled here for the host by
+``tests/sim3_host_harness.cpp``) checked against both on the CPU."""
 
 import os
 import shutil
@@ -160,3 +161,45 @@ def test_device_retraction_matches_oracle(harness):
     np.testing.assert_allclose(out[:, :3], ref[:, :3], atol=2e-6)
     np.testing.assert_allclose(out[:, 7], ref[:, 7], rtol=2e-6)
     np.testing.assert_allclose(quat_align(out[:, 3:7], ref[:, 3:7]), ref[:, 3:7], atol=2e-6)
+
+
+# ------------------------------------------------------------------ the reference's own procedure
+GOLDEN = sorted(__import__("glob").glob(os.path.join(HERE, "golden", "pgo_*.npz")))
+
+
+def _golden(path):
+    z = np.load(path)
+    return {k: z[k] for k in z.files}
+
+
+def test_golden_fixtures_present():
+    assert {os.path.basename(p) for p in GOLDEN} >= {"pgo_frontend_small.npz", "pgo_frontend40.npz"}
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_matches_reference_procedure(path):
+    """oracle vs pgo_buffer.py's own num_jacobi / global_relative_posesim3_constraints
+    (tests/golden/make_golden_pgo.py)."""
+    g = _golden(path)
+    H, v, c2, c2s, _, _, _ = pgo.relative_constraints(g["iip"], g["jjp"], g["poses"], g["rel"], g["infos"],
+                                                      float(g["pw"]))
+    Hf, vf = g["Hsp"][:, 0], g["vsp"][:, 0]
+    assert np.abs(H - Hf).max() < 2e-6 * np.abs(Hf).max()
+    assert np.abs(v - vf).max() < 2e-6 * np.abs(vf).max()
+    np.testing.assert_allclose([c2, c2s], [g["chi2"], g["chi2_scaled"]], rtol=1e-6)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_device_code_matches_reference_procedure(harness, path):
+    g = _golden(path)
+    N, Np = len(g["poses"]), len(g["iip"])
+    _, Hsp, vsp, chi = harness(
+        "factors", [np.array([N, Np], np.int64), g["poses"].astype(np.float32), g["iip"].astype(np.int64),
+                    g["jjp"].astype(np.int64), g["rel"].astype(np.float32), g["infos"].astype(np.float32),
+                    np.array([float(g["pw"])])],
+        [Np * 15 * 7, 4 * Np * 49, 2 * Np * 7, 2 * Np], [np.float64, np.float32, np.float32, np.float32])
+    Hf, vf = g["Hsp"][:, 0], g["vsp"][:, 0]
+    assert np.abs(Hsp.reshape(4, Np, 7, 7) - Hf).max() < 2e-6 * np.abs(Hf).max()
+    assert np.abs(vsp.reshape(2, Np, 7) - vf).max() < 2e-6 * np.abs(vf).max()
+    np.testing.assert_allclose(chi.reshape(Np, 2).astype(np.float64).sum(0), [g["chi2"], g["chi2_scaled"]],
+                               rtol=1e-6)
