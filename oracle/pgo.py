@@ -36,14 +36,25 @@ def quat_to_rot(q):
 
 
 def rot_to_quat(R):
-    w = np.sqrt(max(0.0, 1 + R[0, 0] + R[1, 1] + R[2, 2])) / 2
-    x = np.sqrt(max(0.0, 1 + R[0, 0] - R[1, 1] - R[2, 2])) / 2
-    y = np.sqrt(max(0.0, 1 - R[0, 0] + R[1, 1] - R[2, 2])) / 2
-    z = np.sqrt(max(0.0, 1 - R[0, 0] - R[1, 1] + R[2, 2])) / 2
-    x = np.copysign(x, R[2, 1] - R[1, 2])
-    y = np.copysign(y, R[0, 2] - R[2, 0])
-    z = np.copysign(z, R[1, 0] - R[0, 1])
-    return np.array([x, y, z, w])
+    """Unit quaternion (x y z w, w >= 0) of a rotation matrix by Shepperd's method: the
+    largest of 4w^2, 4x^2, 4y^2, 4z^2 from the diagonal, the others from off-diagonal sums
+    divided by it, so small components keep full relative accuracy."""
+    tr = R[0, 0] + R[1, 1] + R[2, 2]
+    k = int(np.argmax([tr, R[0, 0], R[1, 1], R[2, 2]]))
+    if k == 0:
+        w = np.sqrt(1 + tr) / 2
+        q = [(R[2, 1] - R[1, 2]) / (4 * w), (R[0, 2] - R[2, 0]) / (4 * w), (R[1, 0] - R[0, 1]) / (4 * w), w]
+    elif k == 1:
+        x = np.sqrt(1 + 2 * R[0, 0] - tr) / 2
+        q = [x, (R[0, 1] + R[1, 0]) / (4 * x), (R[0, 2] + R[2, 0]) / (4 * x), (R[2, 1] - R[1, 2]) / (4 * x)]
+    elif k == 2:
+        y = np.sqrt(1 + 2 * R[1, 1] - tr) / 2
+        q = [(R[0, 1] + R[1, 0]) / (4 * y), y, (R[1, 2] + R[2, 1]) / (4 * y), (R[0, 2] - R[2, 0]) / (4 * y)]
+    else:
+        z = np.sqrt(1 + 2 * R[2, 2] - tr) / 2
+        q = [(R[0, 2] + R[2, 0]) / (4 * z), (R[1, 2] + R[2, 1]) / (4 * z), z, (R[1, 0] - R[0, 1]) / (4 * z)]
+    q = np.array(q)
+    return -q if q[3] < 0 else q
 
 
 def to_matrix(p):
