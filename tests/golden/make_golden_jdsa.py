@@ -39,6 +39,8 @@ CASES = {
     "jdsa_tiny6_2x2": dict(name="tiny6", hs=2, ws=2, alpha=0.01),
     # a finer 3x4 grid (several interpolation cells), alpha 0.001 (the Replica config)
     "jdsa_tiny6_3x4": dict(name="tiny6", hs=3, ws=4, alpha=0.001),
+    # a 4x4 grid: 16 scale unknowns per frame, the most the kernel takes
+    "jdsa_tiny6_4x4": dict(name="tiny6", hs=4, ws=4, alpha=0.01),
     # source frames {0, 1, 3, 4, 5}: keys kx - kx[0] skip 2, so one block gets no prior
     # terms, key 5 is dropped by safe_scatter_add_mat, and blocks 3 and 4 pair the prior
     # terms of frames 3 and 4 with the rows (C, w, mask) of frames 4 and 5.  A prior on

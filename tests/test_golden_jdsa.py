@@ -29,7 +29,7 @@ def rel(a, b):
 
 def test_fixtures_present():
     names = {os.path.basename(p)[:-4] for p in CASES}
-    assert {"jdsa_tiny6_2x2", "jdsa_tiny6_3x4", "jdsa_tiny6_gap", "jdsa_tiny6_gap_fails",
+    assert {"jdsa_tiny6_2x2", "jdsa_tiny6_3x4", "jdsa_tiny6_4x4", "jdsa_tiny6_gap", "jdsa_tiny6_gap_fails",
             "jdsa_tiny7_offset"} <= names
 
 
