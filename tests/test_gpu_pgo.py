@@ -2,6 +2,8 @@
 (``oracle/pgo.py``), and the pgba loop of ``DepthVideo.cuda_pgba`` on the GPU against the
 oracle chain."""
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -116,3 +118,16 @@ def test_cuda_pgba_loop_matches_oracle_chain(cuda):
     np.testing.assert_allclose(out[:, :3], P[:, :3], atol=1e-4 * np.abs(P[:, :3]).max())
     np.testing.assert_allclose(out[:, 7], P[:, 7], rtol=1e-4)
     assert _rel(disps.cpu().numpy(), D) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["pgo_frontend_small", "pgo_frontend40"])
+def test_constraints_match_reference_procedure(cuda, name):
+    """Against pgo_buffer.py's own num_jacobi / global_relative_posesim3_constraints
+    (fixtures made by tests/golden/make_golden_pgo.py)."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    f = lambda k, dt=torch.float32: torch.tensor(z[k], dtype=dt, device=cuda).contiguous()  # noqa: E731
+    Hsp, vsp, chi2, chi2s = pgo.global_relative_posesim3_constraints(
+        f("iip", torch.int64), f("jjp", torch.int64), f("poses")[None], f("rel")[None], f("infos"), pw=float(z["pw"]))
+    assert _rel(Hsp.cpu().numpy(), z["Hsp"]) < 1e-5
+    assert _rel(vsp.cpu().numpy(), z["vsp"]) < 1e-5
+    np.testing.assert_allclose([float(chi2), float(chi2s)], [z["chi2"], z["chi2_scaled"]], rtol=1e-5)
