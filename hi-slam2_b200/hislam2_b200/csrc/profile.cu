@@ -5,6 +5,7 @@
 // recorded events, sums the elapsed time per kernel name and returns one line
 // per kernel: "<name> <launches> <total_ms>".  Disabled (the default), the
 // bracketing costs one branch per launch.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -22,7 +23,7 @@ struct Rec {
   cudaEvent_t start, stop;
 };
 std::mutex g_mu;
-bool g_enabled = false;
+std::atomic<bool> g_enabled{false};   // read without the lock on every launch
 std::vector<Rec> g_recs;        // recorded pairs since the last reset
 std::vector<cudaEvent_t> g_pool;  // spare events
 }  // namespace
@@ -39,7 +40,7 @@ static cudaEvent_t take_event() {
 }
 
 ProfScope::ProfScope(const char* name, cudaStream_t s) : name_(name), stream_(s), start_(nullptr) {
-  if (!g_enabled) return;
+  if (!g_enabled.load(std::memory_order_relaxed)) return;
   std::lock_guard<std::mutex> lk(g_mu);
   start_ = take_event();
   if (start_) cudaEventRecord(start_, stream_);
@@ -57,8 +58,7 @@ ProfScope::~ProfScope() {
 }  // namespace hs2
 
 extern "C" void hs2_profile_enable(int on) {
-  std::lock_guard<std::mutex> lk(hs2::g_mu);
-  hs2::g_enabled = on != 0;
+  hs2::g_enabled.store(on != 0, std::memory_order_relaxed);
 }
 
 extern "C" int hs2_profile_report(char* buf, size_t len, int reset) {
